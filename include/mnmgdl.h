@@ -1,0 +1,190 @@
+/*
+ * mnmgdl.h -- C-ABI of the B200 semi-naive Datalog engine (libmnmgdl.so).
+ *
+ * Plain C types only: device pointers are `void *` / `dl_entity *`, sizes are
+ * int64_t, streams are `cudaStream_t` passed as `void *`. Every entry point
+ * returns a dl_status; on failure dl_last_error() gives a message for the
+ * calling thread. Device-side waits are bounded: a wait that runs out returns
+ * DL_ERR_DEVICE_TIMEOUT instead of hanging.
+ *
+ * Reference interface each group replaces (paths within harp-lab/MNMGDatalog):
+ *   dl_build_hash_table      <- get_hash_table            common/hash_table.cu:24-55
+ *   dl_join                  <- get_join                  common/join.cu:51-87
+ *   dl_join_sorted           <- get_join_nl               common/join.cu:144-180
+ *   dl_sort_unique           <- thrust::sort(set_cmp) + thrust::unique(is_equal)   tc.cu:250-253
+ *   dl_set_difference        <- thrust::set_difference(set_cmp)                    tc.cu:260-263
+ *   dl_merge                 <- thrust::merge(set_cmp)                             tc.cu:276-279
+ *   dl_unique_by_key_min     <- thrust::unique(is_equal_key) on set_cmp order       wcc.cu:320-323
+ *   dl_remove_self_pairs     <- thrust::remove_if(is_key_equal_value)              sg.cu:176-179
+ *   dl_diff_merge            <- set_difference + merge pair of one iteration       tc.cu:260-286
+ *   dl_run_program / dl_run_tc / dl_run_sg / dl_run_wcc / dl_run_single_join
+ *                            <- the program drivers       tc.cu:42-423, sg.cu:40-477,
+ *                                                          wcc.cu:58-585, single_join.cu:39-396
+ *   dl_generate_rows         <- parallel_generate         common/parallel_io.cu:79-108
+ * The reference's exact C++ signatures (Entity*, int sizes, exit on error)
+ * are provided on top of this ABI by include/mnmgdl_compat.h.
+ */
+#ifndef MNMGDL_H
+#define MNMGDL_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define DL_API __attribute__((visibility("default")))
+#else
+#define DL_API
+#endif
+
+typedef enum dl_status {
+    DL_OK = 0,
+    DL_ERR_INVALID_ARGUMENT = 1,
+    DL_ERR_CUDA = 2,
+    DL_ERR_OUT_OF_MEMORY = 3,
+    DL_ERR_DEVICE_TIMEOUT = 4,
+    DL_ERR_OVERFLOW = 5,
+    DL_ERR_NO_DEVICE = 6,
+    DL_ERR_INTERNAL = 7
+} dl_status;
+
+/* Same layout as the reference's Entity (common/utils.cu:8-11). Relations
+ * are ordered by the reference's set_cmp: signed key, then signed value. */
+typedef struct dl_entity {
+    int32_t key;
+    int32_t value;
+} dl_entity;
+
+typedef struct dl_context dl_context;
+typedef struct dl_hash_table dl_hash_table;
+typedef struct dl_run dl_run;
+
+typedef enum dl_program {
+    DL_PROGRAM_TC = 0,          /* path(x,z) :- path(x,y), edge(y,z)          tc.cu */
+    DL_PROGRAM_SG = 1,          /* same generation                            sg.cu */
+    DL_PROGRAM_WCC = 2,         /* weakly connected components (min label)    wcc.cu */
+    DL_PROGRAM_SINGLE_JOIN = 3  /* R(a,b), R(b,c) -> (a,c), deduplicated       single_join.cu */
+} dl_program;
+
+typedef enum dl_wcc_stop {
+    /* Stop when |delta_k| == |delta_{k-1}| (wcc.cu:366-383): bit-exact with
+     * the reference, including its early stop on some graphs. */
+    DL_WCC_STOP_REFERENCE = 0,
+    /* Stop when |delta_k| == 0: the true connected components. */
+    DL_WCC_STOP_FIXPOINT = 1
+} dl_wcc_stop;
+
+typedef struct dl_options {
+    int32_t wcc_stop;        /* dl_wcc_stop */
+    int32_t max_iterations;  /* 0 = run to the fixpoint */
+    int32_t phase_timing;    /* 1 = record per-phase device times (adds events) */
+    int32_t reserved[5];
+} dl_options;
+
+typedef struct dl_run_info {
+    int32_t program;             /* dl_program */
+    int32_t iterations;          /* counted like the reference (final empty pass included) */
+    int64_t input_rows;
+    int64_t output_rows;         /* rows of the program's output file */
+    int64_t output_tuples;       /* TC/SG/single_join: |result|; WCC: # components */
+    int64_t largest_component;   /* WCC only */
+    int64_t nodes;               /* distinct node ids in the input */
+    double seconds_total;        /* device time, H2D of the input through the last iteration */
+    double seconds_init;         /* phase times (phase_timing = 1), reference CSV columns */
+    double seconds_join;
+    double seconds_dedup;
+    double seconds_merge;
+    double seconds_finalize;
+} dl_run_info;
+
+DL_API const char *dl_status_string(dl_status s);
+DL_API const char *dl_last_error(void);
+DL_API const char *dl_version(void);
+
+/* Context: one CUDA device + stream (NULL = a stream owned by the context). */
+DL_API dl_status dl_context_create(int32_t device, void *stream, dl_context **out);
+DL_API dl_status dl_context_destroy(dl_context *ctx);
+DL_API dl_status dl_context_synchronize(dl_context *ctx);
+DL_API dl_status dl_free(dl_context *ctx, void *device_ptr);
+/* Copy `bytes` between any two host/device buffers on the context's stream
+ * and wait for it (cudaMemcpyDefault). */
+DL_API dl_status dl_memcpy(dl_context *ctx, void *dst, const void *src, int64_t bytes);
+
+/* ---- relational operators on device arrays of dl_entity (set_cmp order) ---- */
+
+/* Sort in place and drop duplicates; *n_out = new length. */
+DL_API dl_status dl_sort_unique(dl_context *ctx, dl_entity *rel, int64_t n, int64_t *n_out);
+/* Sort in place (duplicates kept). */
+DL_API dl_status dl_sort(dl_context *ctx, dl_entity *rel, int64_t n);
+/* out = a \ b for sorted duplicate-free a and b; out may alias a. */
+DL_API dl_status dl_set_difference(dl_context *ctx, const dl_entity *a, int64_t na, const dl_entity *b,
+                                   int64_t nb, dl_entity *out, int64_t *n_out);
+/* out = stable merge of sorted a and b, duplicates kept (ties: a first). */
+DL_API dl_status dl_merge(dl_context *ctx, const dl_entity *a, int64_t na, const dl_entity *b, int64_t nb,
+                          dl_entity *out);
+/* One semi-naive step on sets: delta_out = dedup(j) \ full, full_out = full u j.
+ * full sorted duplicate-free, j sorted (duplicates allowed). full_out holds
+ * nfull + *n_delta rows afterwards. Either output may be NULL. */
+DL_API dl_status dl_diff_merge(dl_context *ctx, const dl_entity *full, int64_t nfull, const dl_entity *j,
+                               int64_t nj, dl_entity *full_out, dl_entity *delta_out, int64_t *n_delta);
+/* Keep the first row of every key run of a sorted relation (= minimum value). */
+DL_API dl_status dl_unique_by_key_min(dl_context *ctx, dl_entity *rel, int64_t n, int64_t *n_out);
+/* Drop rows with key == value, order kept. */
+DL_API dl_status dl_remove_self_pairs(dl_context *ctx, dl_entity *rel, int64_t n, int64_t *n_out);
+
+/* ---- hash table and joins ---- */
+
+/* Index a relation by key. load_factor <= 0 selects the default (0.5). The
+ * table keeps its own copy; rel may be freed afterwards. */
+DL_API dl_status dl_build_hash_table(dl_context *ctx, const dl_entity *rel, int64_t n, double load_factor,
+                                     dl_hash_table **out);
+DL_API dl_status dl_hash_table_info(const dl_hash_table *ht, int64_t *slots, int64_t *distinct_keys,
+                                    int64_t *rows);
+DL_API dl_status dl_hash_table_destroy(dl_hash_table *ht);
+/* For every probe row (k, v) and every indexed row (k, w) emit (w, v).
+ * *out is a new device buffer of *n_out rows (NULL when empty); release it
+ * with dl_free. Rows are grouped by probe row, probe order kept. */
+DL_API dl_status dl_join(dl_context *ctx, const dl_hash_table *ht, const dl_entity *probe, int64_t n,
+                         dl_entity **out, int64_t *n_out);
+/* Same result through binary search of a key-sorted relation. */
+DL_API dl_status dl_join_sorted(dl_context *ctx, const dl_entity *sorted_rel, int64_t n_rel,
+                                const dl_entity *probe, int64_t n, dl_entity **out, int64_t *n_out);
+
+/* ---- programs ---- */
+
+/* Run one program on an edge relation of `rows` int32 pairs (the binary
+ * edge-file layout). `edges_on_device` = 1 if `edges` is device memory.
+ * For DL_PROGRAM_SINGLE_JOIN the pairs are the relation R. */
+DL_API dl_status dl_run_program(dl_context *ctx, int32_t program, const int32_t *edges, int64_t rows,
+                                int32_t edges_on_device, const dl_options *opts, dl_run **out);
+DL_API dl_status dl_run_tc(dl_context *ctx, const int32_t *edges, int64_t rows, int32_t edges_on_device,
+                           const dl_options *opts, dl_run **out);
+DL_API dl_status dl_run_sg(dl_context *ctx, const int32_t *edges, int64_t rows, int32_t edges_on_device,
+                           const dl_options *opts, dl_run **out);
+DL_API dl_status dl_run_wcc(dl_context *ctx, const int32_t *edges, int64_t rows, int32_t edges_on_device,
+                            const dl_options *opts, dl_run **out);
+DL_API dl_status dl_run_single_join(dl_context *ctx, const int32_t *rel, int64_t rows, int32_t rel_on_device,
+                                    const dl_options *opts, dl_run **out);
+DL_API dl_status dl_run_get_info(const dl_run *run, dl_run_info *info);
+/* Output rows exactly as the reference writes its output file:
+ * TC (x,z) ordered by (z,x); SG (x,y) ordered by (x,y); WCC (component,0)
+ * ascending; single_join (a,c) ordered by (c,a). dst holds capacity_rows
+ * int32 pairs, host memory unless dst_on_device = 1. */
+DL_API dl_status dl_run_copy_output(const dl_run *run, int32_t *dst, int64_t capacity_rows,
+                                    int32_t dst_on_device);
+/* |delta| after each iteration (length = iterations). */
+DL_API dl_status dl_run_copy_deltas(const dl_run *run, int64_t *dst, int64_t capacity);
+/* WCC: every node id (ascending) and its final component label. */
+DL_API dl_status dl_run_copy_labels(const dl_run *run, int32_t *node_ids, int32_t *labels, int64_t capacity);
+DL_API dl_status dl_run_destroy(dl_run *run);
+
+/* The reference's synthetic single-join rows: C library srand(seed) then
+ * rand() % rand_range + 1 for 2*rows values (glibc generator). */
+DL_API dl_status dl_generate_rows(int64_t rows, int32_t rand_range, uint32_t seed, int32_t *host_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

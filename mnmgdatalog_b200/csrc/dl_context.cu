@@ -1,0 +1,116 @@
+// Context: device, stream, control block, grow-only scratch.
+#include "dl_internal.h"
+
+namespace dl {
+
+void DevBuf::reserve(size_t bytes, bool zero) {
+    if (bytes <= cap && p) return;
+    size_t want = bytes + bytes / 8 + 256;
+    release();
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cap = 0;
+        (void) cudaGetLastError();
+        throw Error(DL_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(want) + " bytes failed: " +
+                                              cudaGetErrorString(e));
+    }
+    cap = want;
+    if (zero) DL_CUDA(cudaMemset(p, 0, want));
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+
+void Context::reserve(DevBuf &buf, size_t bytes, bool zero) {
+    if (buf.p && buf.cap >= bytes) return;
+    int best = -1;
+    for (int i = 0; i < (int) spares.size(); ++i)
+        if (spares[i].cap >= bytes && (best < 0 || spares[i].cap < spares[best].cap)) best = i;
+    if (best >= 0) {
+        buf.release();
+        buf = spares[best];
+        spares.erase(spares.begin() + best);
+        if (zero) DL_CUDA(cudaMemsetAsync(buf.p, 0, buf.cap, stream));
+        return;
+    }
+    if (buf.p) {
+        // Keep the old allocation for smaller requests later.
+        spares.push_back(buf);
+        buf = DevBuf();
+    }
+    try {
+        buf.reserve(bytes, zero);
+    } catch (const Error &) {
+        // Out of memory: drop every spare and retry once.
+        for (auto &s : spares) s.release();
+        spares.clear();
+        buf.reserve(bytes, zero);
+    }
+}
+
+void Context::give_back(DevBuf &buf) {
+    if (!buf.p) return;
+    spares.push_back(buf);
+    buf = DevBuf();
+    while (spares.size() > 6) {
+        // Free the smallest spare.
+        int small = 0;
+        for (int i = 1; i < (int) spares.size(); ++i)
+            if (spares[i].cap < spares[small].cap) small = i;
+        spares[small].release();
+        spares.erase(spares.begin() + small);
+    }
+}
+
+void Context::release_all() {
+    for (auto &s : spares) s.release();
+    spares.clear();
+    DevBuf *all[] = {&ws.input, &ws.ids, &ws.w0, &ws.w1, &ws.csr_off, &ws.csr_val, &ws.full[0], &ws.full[1],
+                     &ws.jbuf[0], &ws.jbuf[1], &ws.offsets, &ws.wcc_label, &ws.wcc_flag, &ws.wcc_next,
+                     &lookback, &sort_hist, &lbs_splits};
+    for (DevBuf *b : all) b->release();
+}
+
+u32 Context::next_epoch() {
+    if (epoch >= kEpochMask) {
+        // Wrap: clear every word so none can carry a recycled epoch.
+        if (lookback.p) DL_CUDA(cudaMemsetAsync(lookback.p, 0, lookback.cap, stream));
+        epoch = 0;
+    }
+    return ++epoch;
+}
+
+u64 *Context::lookback_words(size_t words) {
+    if (words * sizeof(u64) > lookback.cap) {
+        sync();
+        lookback.reserve(words * sizeof(u64), true);
+    }
+    return lookback.as<u64>();
+}
+
+u32 *Context::tile_counter(int slot) { return &ctrl->tile_counter[slot]; }
+
+void Context::check_device_error() {
+    u32 err = reinterpret_cast<volatile u32 *>(host_scalars)[2 * 63];
+    if (err) {
+        DL_CUDA(cudaMemsetAsync(&ctrl->err, 0, sizeof(u32), stream));
+        DL_CUDA(cudaStreamSynchronize(stream));
+        reinterpret_cast<volatile u32 *>(host_scalars)[2 * 63] = 0;
+        if (err & DL_DEVERR_LOOKBACK)
+            throw Error(DL_ERR_DEVICE_TIMEOUT, "a device-side wait exceeded its limit (decoupled look-back)");
+        throw Error(DL_ERR_INTERNAL, "device error flag " + std::to_string(err));
+    }
+}
+
+void Context::sync() {
+    DL_CUDA(cudaMemcpyAsync(reinterpret_cast<u32 *>(host_scalars) + 2 * 63, &ctrl->err, sizeof(u32),
+                            cudaMemcpyDeviceToHost, stream));
+    DL_CUDA(cudaStreamSynchronize(stream));
+    check_device_error();
+}
+
+}  // namespace dl

@@ -1,0 +1,28 @@
+// Program runs (dl_run) of the engine; see dl_engine.cu.
+#pragma once
+
+#include "dl_internal.h"
+
+namespace dl {
+
+struct Run {
+    Context *ctx = nullptr;
+    dl_program program = DL_PROGRAM_TC;
+    dl_run_info info{};
+    std::vector<i64> deltas;  // |delta| after each iteration
+    DevBuf words;             // TC/SG/single_join: sorted result words
+    u64 n_words = 0;
+    DevBuf ids;               // node id of each rank
+    u32 n_ids = 0;
+    int bits = 1;             // bits per rank in a word
+    DevBuf aux;               // WCC: component ranks, ascending
+    u64 n_aux = 0;
+    DevBuf labels;            // WCC: label rank of every node
+};
+
+Run *run_program(Context &ctx, int program, const int32_t *rows, u64 n, bool on_device, const dl_options &opt);
+void run_copy_output(const Run &r, int32_t *dst, u64 capacity, bool dst_on_device);
+void run_copy_labels(const Run &r, int32_t *node_ids, int32_t *labels, u64 capacity);
+void run_destroy(Run *r);
+
+}  // namespace dl

@@ -1,0 +1,140 @@
+// Host-side internals shared by the engine's translation units (not part of
+// the C-ABI; see include/mnmgdl.h for that).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/mnmgdl.h"
+#include "dl_device.cuh"
+
+namespace dl {
+
+// Error raised inside the engine; the C-ABI layer converts it to a dl_status.
+struct Error : std::runtime_error {
+    dl_status status;
+    Error(dl_status s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+#define DL_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            throw ::dl::Error(e_ == cudaErrorMemoryAllocation ? DL_ERR_OUT_OF_MEMORY : DL_ERR_CUDA, \
+                              std::string(#call) + ": " + cudaGetErrorString(e_));             \
+        }                                                                                      \
+    } while (0)
+
+#define DL_CHECK_LAUNCH() DL_CUDA(cudaGetLastError())
+
+// Grow-only device buffer; no allocation happens inside a fixpoint iteration
+// once the capacities have reached their high-water mark.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    void reserve(size_t bytes, bool zero = false);
+    void release();
+    template <typename T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// Engine scratch reused across runs of one context (capacities only grow).
+struct Workspace {
+    DevBuf input;          // device copy of host edge rows
+    DevBuf ids;            // sorted distinct node ids (int32)
+    DevBuf w0, w1;         // word buffers for the initial sorts
+    DevBuf csr_off, csr_val;
+    DevBuf full[2];        // full relation, ping-pong
+    DevBuf jbuf[2];        // join output / sort ping-pong / delta
+    DevBuf offsets;        // join count offsets
+    DevBuf wcc_label, wcc_flag, wcc_next;
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 148;
+    Ctrl *ctrl = nullptr;           // device control block
+    u32 epoch = 0;                  // look-back epoch of the last launch
+    DevBuf lookback;                // look-back words (zeroed at allocation)
+    DevBuf sort_hist;               // radix histograms / bucket bases
+    DevBuf lbs_splits;              // join emit partition points
+    u64 *host_scalars = nullptr;    // pinned mirror for small D2H reads
+    Workspace ws;
+    std::vector<DevBuf> spares;     // buffers handed back by destroyed runs
+
+    // Ensure buf holds `bytes`, preferring a spare buffer over cudaMalloc.
+    void reserve(DevBuf &buf, size_t bytes, bool zero = false);
+    void give_back(DevBuf &buf);
+    void release_all();
+
+    // Next look-back epoch; clears the look-back buffer when the 14-bit epoch
+    // wraps so that no stale word can alias the current launch.
+    u32 next_epoch();
+    // Look-back buffer with room for `words` words.
+    u64 *lookback_words(size_t words);
+    // Tile counter `slot` (reset to zero on the stream before use).
+    u32 *tile_counter(int slot);
+    void check_device_error();
+    void sync();
+};
+
+// ---- radix sort (dl_radix.cu) ----------------------------------------------
+enum class Codec { Raw = 0, Entity = 1 };
+// Sorts n keys from `a` (using `b` as the ping-pong buffer) in ascending
+// order. If `known_bits` > 0 only digits covering bits [0, known_bits) are
+// sorted (keys must be zero above that); otherwise a histogram pass finds the
+// digits that vary (one host read). Returns the buffer holding the result.
+u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits,
+                u64 *hist_accumulated = nullptr);
+// Histogram of the digits [0, ndigits) accumulated by producers (join emit)
+// into ctx.sort_hist; lets radix_sort skip its own histogram pass.
+u64 *radix_hist_buffer(Context &ctx);
+void radix_hist_clear(Context &ctx);
+
+// ---- compaction / scan (dl_scan.cu) ------------------------------------------
+// out[i] = in[i] for the first of each run of equal words; returns count.
+// `out` may alias `in`. With `by_key_shift` < 64, words compare on bits
+// >= by_key_shift only (unique by key, keeps the first = smallest value).
+u64 unique_words(Context &ctx, const u64 *in, u64 n, u64 *out, int by_key_shift = 64,
+                 Codec codec = Codec::Raw);
+// Drops entity words whose key equals value. `out` may alias `in`.
+u64 remove_self_pairs_words(Context &ctx, const u64 *in, u64 n, u64 *out);
+
+// ---- merge path (dl_setops.cu) -------------------------------------------------
+// Stable merge (ties take `a` first), keeps duplicates: thrust::merge.
+void merge_words(Context &ctx, const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, Codec codec);
+// full_out = unique(merge(full, j)); delta_out = (j \ full) deduplicated.
+// `j` sorted (duplicates allowed), `full` sorted unique. Either output may be
+// null. Returns |delta|. full_out receives |full| + |delta| words.
+u64 diff_merge_words(Context &ctx, const u64 *full, u64 nfull, const u64 *j, u64 nj,
+                     u64 *full_out, u64 *delta_out, Codec codec);
+
+// ---- joins (dl_join.cu) --------------------------------------------------------
+struct Csr {            // relation grouped by dense key index
+    u32 *off = nullptr; // n_keys + 1 offsets into val
+    u32 *val = nullptr; // value indices
+    u32 n_keys = 0;
+    u64 n_vals = 0;
+};
+enum class EmitKind : int {
+    ZV = 0,        // (z, v): TC, WCC-style
+    VZ = 1,        // (v, z): join + column swap fused (SG rules)
+    ZV_NOSELF = 2, // (z, v) with z == v replaced by an all-ones word (SG base)
+};
+// Join probe words (k << bits | v) against the CSR: every match (k, z)
+// emits one word per EmitKind. Returns the number of words written to
+// `out` (which must hold the count returned by join_count). `offsets` holds
+// n_probe u64 exclusive offsets computed by join_count.
+u64 join_count(Context &ctx, const Csr &csr, const u64 *probe, u64 n_probe, int bits, u64 *offsets);
+void join_emit(Context &ctx, const Csr &csr, const u64 *probe, u64 n_probe, int bits, const u64 *offsets,
+               u64 total, EmitKind kind, u64 *out, u64 *hist, int hist_digits, u64 *self_pairs);
+
+}  // namespace dl

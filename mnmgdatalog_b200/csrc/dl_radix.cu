@@ -1,0 +1,246 @@
+// LSD radix sort of 64-bit tuple words (the dedup step's sort).
+//
+// Replaces thrust::sort(set_cmp) on Entity arrays (tc.cu:250-253,
+// sg.cu:282-287, wcc.cu:286-291), which dispatches to a comparison merge
+// sort. Here every pass is one "onesweep" kernel: a tile of 6144 keys is
+// ranked by 8-bit digit inside the CTA (warp ballots + per-warp counters,
+// stable), the tile's digit counts are chained to earlier tiles by
+// decoupled look-back, and the keys leave through shared memory so that the
+// global writes of one digit run are contiguous. Only digits whose bits vary
+// are sorted: the engine's compact words carry 2*B bits (B = bits per node
+// index), the C-ABI path detects constant digits from the histogram.
+//
+// HBM traffic per pass: 8 B read + 8 B written per key (+ 8 B read once for
+// the histogram unless a producer kernel accumulated it while writing).
+#include "dl_internal.h"
+
+namespace dl {
+namespace {
+
+constexpr int RADIX = 256;
+constexpr int SORT_THREADS = 384;
+constexpr int SORT_WARPS = SORT_THREADS / 32;
+constexpr int SORT_KPT = 16;
+constexpr int SORT_TILE = SORT_THREADS * SORT_KPT;  // 6144 keys, 48 KiB
+constexpr int HIST_THREADS = 512;
+
+struct SortSmem {
+    u64 keys[SORT_TILE];
+    u32 warp_cnt[SORT_WARPS][RADIX];
+    u64 gbase[RADIX];
+    u32 tile_start[RADIX];
+    u32 scratch[SORT_WARPS + 1];
+    u32 tile;
+};
+
+template <bool ENC>
+__global__ void __launch_bounds__(HIST_THREADS)
+radix_hist_kernel(const u64 *__restrict__ keys, u64 n, int ndig, u64 *__restrict__ hist) {
+    __shared__ u32 sh[8 * RADIX];
+    for (int i = threadIdx.x; i < 8 * RADIX; i += HIST_THREADS) sh[i] = 0;
+    __syncthreads();
+    const u64 stride = (u64) gridDim.x * HIST_THREADS;
+    for (u64 i = (u64) blockIdx.x * HIST_THREADS + threadIdx.x; i < n; i += stride) {
+        u64 k = __ldcs(keys + i);
+        if (ENC) k = entity_encode(k);
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
+            if (d < ndig) atomicAdd(&sh[d * RADIX + ((k >> (8 * d)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ndig * RADIX; i += HIST_THREADS) {
+        u32 c = sh[i];
+        if (c) atomicAdd((unsigned long long *) &hist[i], (unsigned long long) c);
+    }
+}
+
+// One block per digit: bucket[d][b] = exclusive scan of hist[d][*]; marks the
+// digits on which all keys agree (nothing to sort).
+__global__ void __launch_bounds__(RADIX) radix_bucket_kernel(const u64 *__restrict__ hist, u64 *__restrict__ bucket,
+                                                             u64 n, u32 *trivial_mask) {
+    __shared__ u64 scratch[RADIX / 32 + 1];
+    const int d = blockIdx.x;
+    u64 c = hist[d * RADIX + threadIdx.x];
+    u64 tot;
+    u64 ex = block_exclusive_sum<RADIX / 32>(c, scratch, &tot);
+    bucket[d * RADIX + threadIdx.x] = ex;
+    if (c == n) atomicOr(trivial_mask, 1u << d);
+}
+
+template <bool ENC, bool DEC>
+__global__ void __launch_bounds__(SORT_THREADS, 2)
+onesweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int shift,
+                const u64 *__restrict__ bucket, u64 *lb, u32 *tile_ctr, u32 epoch, u32 *err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem &s = *reinterpret_cast<SortSmem *>(smem_raw);
+    const int tid = threadIdx.x;
+    const u32 lane = tid & 31;
+    const int w = tid >> 5;
+
+    for (int i = tid; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&s.warp_cnt[0][0])[i] = 0;
+    if (tid == 0) s.tile = atomicAdd(tile_ctr, 1u);
+    __syncthreads();
+    const u32 tile = s.tile;
+    const u64 tile_base = (u64) tile * SORT_TILE;
+    const u32 n_valid = (u32) min((u64) SORT_TILE, n - tile_base);
+
+    // Warp-contiguous blocks, lane-striped items: coalesced 256 B loads, and
+    // (warp, item, lane) order equals input order, which keeps ranks stable.
+    u64 k[SORT_KPT];
+    const u64 wbase = tile_base + (u64) w * 32 * SORT_KPT + lane;
+#pragma unroll
+    for (int i = 0; i < SORT_KPT; ++i) {
+        const u64 idx = wbase + (u64) i * 32;
+        if (idx < n) {
+            u64 x = __ldcs(in + idx);
+            k[i] = ENC ? entity_encode(x) : x;
+        } else {
+            k[i] = ~0ull;  // ranks after every valid key of digit 255
+        }
+    }
+
+    u32 rank[SORT_KPT];
+    const u32 lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < SORT_KPT; ++i) {
+        const u32 d = (u32) (k[i] >> shift) & 255u;
+        u32 peers = 0xffffffffu;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const u32 bit = (d >> b) & 1u;
+            const u32 bal = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? bal : ~bal;
+        }
+        const u32 leader = __ffs(peers) - 1;
+        u32 prev = 0;
+        if (lane == leader) {
+            prev = s.warp_cnt[w][d];
+            s.warp_cnt[w][d] = prev + __popc(peers);
+        }
+        __syncwarp();
+        prev = __shfl_sync(0xffffffffu, prev, leader);
+        rank[i] = prev + __popc(peers & lt);
+    }
+    __syncthreads();
+
+    u32 cnt_all = 0, cnt_valid = 0;
+    if (tid < RADIX) {
+        u32 sum = 0;
+#pragma unroll
+        for (int ww = 0; ww < SORT_WARPS; ++ww) {
+            const u32 c = s.warp_cnt[ww][tid];
+            s.warp_cnt[ww][tid] = sum;
+            sum += c;
+        }
+        cnt_all = sum;
+        cnt_valid = (tid == RADIX - 1) ? sum - (SORT_TILE - n_valid) : sum;
+        st_relaxed_u64(lb + (u64) tile * RADIX + tid, lb_word(tile == 0 ? kStatusInc : kStatusAgg, epoch, cnt_valid));
+    }
+    u32 total;
+    const u32 start = block_exclusive_sum<SORT_WARPS>(tid < RADIX ? cnt_all : 0u, s.scratch, &total);
+    if (tid < RADIX) {
+        s.tile_start[tid] = start;
+        u64 excl = 0;
+        if (tile > 0) {
+            excl = lookback_serial(lb + tid, tile, RADIX, epoch, err);
+            st_relaxed_u64(lb + (u64) tile * RADIX + tid, lb_word(kStatusInc, epoch, excl + cnt_valid));
+        }
+        s.gbase[tid] = bucket[tid] + excl - start;
+    }
+    __syncthreads();
+
+#pragma unroll
+    for (int i = 0; i < SORT_KPT; ++i) {
+        const u32 d = (u32) (k[i] >> shift) & 255u;
+        s.keys[s.tile_start[d] + s.warp_cnt[w][d] + rank[i]] = k[i];
+    }
+    __syncthreads();
+
+    for (u32 j = tid; j < n_valid; j += SORT_THREADS) {
+        const u64 x = s.keys[j];
+        const u32 d = (u32) (x >> shift) & 255u;
+        out[s.gbase[d] + j] = DEC ? entity_decode(x) : x;
+    }
+}
+
+template <bool ENC, bool DEC>
+void launch_onesweep(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, const u64 *bucket, u64 *lb,
+                     u32 *ctr) {
+    static bool configured = false;
+    auto kern = onesweep_kernel<ENC, DEC>;
+    if (!configured) {
+        DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(SortSmem)));
+        configured = true;
+    }
+    const u64 tiles = (n + SORT_TILE - 1) / SORT_TILE;
+    kern<<<(unsigned) tiles, SORT_THREADS, sizeof(SortSmem), ctx.stream>>>(in, out, n, shift, bucket, lb, ctr,
+                                                                          ctx.next_epoch(), &ctx.ctrl->err);
+    DL_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+// Histogram bins [8][256] followed by bucket bases [8][256].
+u64 *radix_hist_buffer(Context &ctx) {
+    ctx.sort_hist.reserve(2 * 8 * RADIX * sizeof(u64));
+    return ctx.sort_hist.as<u64>();
+}
+
+void radix_hist_clear(Context &ctx) {
+    DL_CUDA(cudaMemsetAsync(radix_hist_buffer(ctx), 0, 8 * RADIX * sizeof(u64), ctx.stream));
+}
+
+u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits, u64 *hist_accumulated) {
+    if (n <= 1) return a;
+    const bool ent = codec == Codec::Entity;
+    u64 *hist = radix_hist_buffer(ctx);
+    u64 *bucket = hist + 8 * RADIX;
+    u32 *ctr = ctx.tile_counter(0);
+    u32 *mask = ctx.tile_counter(16);
+    int digits[8];
+    int nd = 0;
+    DL_CUDA(cudaMemsetAsync(ctr, 0, 17 * sizeof(u32), ctx.stream));
+    const int ndig = (known_bits > 0 && !ent) ? (known_bits + 7) / 8 : 8;
+    const unsigned hgrid = (unsigned) std::min<u64>((n + HIST_THREADS * 8 - 1) / (HIST_THREADS * 8),
+                                                    (u64) ctx.sm_count * 4);
+    if (!hist_accumulated) {
+        radix_hist_clear(ctx);
+        if (ent)
+            radix_hist_kernel<true><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist);
+        else
+            radix_hist_kernel<false><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist);
+        DL_CHECK_LAUNCH();
+    }
+    radix_bucket_kernel<<<ndig, RADIX, 0, ctx.stream>>>(hist, bucket, n, mask);
+    DL_CHECK_LAUNCH();
+    if (known_bits > 0 && !ent) {
+        for (int d = 0; d < ndig; ++d) digits[nd++] = d;
+    } else {
+        u32 m = 0;
+        DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, mask, sizeof(u32), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        m = *reinterpret_cast<u32 *>(ctx.host_scalars);
+        for (int d = 0; d < 8; ++d)
+            if (!((m >> d) & 1u)) digits[nd++] = d;
+    }
+    if (nd == 0) return a;
+    const u64 tiles = (n + SORT_TILE - 1) / SORT_TILE;
+    u64 *lb = ctx.lookback_words(tiles * RADIX);
+    const u64 *src = a;
+    u64 *dst = b;
+    for (int p = 0; p < nd; ++p) {
+        const bool enc = ent && p == 0, dec = ent && p == nd - 1;
+        const u64 *bk = bucket + digits[p] * RADIX;
+        const int sh = 8 * digits[p];
+        if (enc && dec) launch_onesweep<true, true>(ctx, src, dst, n, sh, bk, lb, ctr + p);
+        else if (enc) launch_onesweep<true, false>(ctx, src, dst, n, sh, bk, lb, ctr + p);
+        else if (dec) launch_onesweep<false, true>(ctx, src, dst, n, sh, bk, lb, ctr + p);
+        else launch_onesweep<false, false>(ctx, src, dst, n, sh, bk, lb, ctr + p);
+        u64 *t = const_cast<u64 *>(src);
+        src = dst;
+        dst = t;
+    }
+    return const_cast<u64 *>(src);
+}
+
+}  // namespace dl

@@ -1,0 +1,106 @@
+"""Seeded synthetic edge relations with the shapes of the reference's graphs.
+
+The reference's headline graphs (com-dblp, fe_body, ...) are public datasets
+that are not shipped here; these generators produce int32 edge rows of the
+same scale and degree structure, deterministically from a seed:
+
+* ``dag``        -- a DAG on 0..n-1: edge i->i+1 with probability p, plus
+                    `extra` edges u->v, v uniform in (u, u+span]; duplicates
+                    removed (the OL.cedge-scale TC input, ~5.5K edges).
+* ``chung_lu``   -- a Chung-Lu power-law graph (expected degrees ~ rank^(-1/(gamma-1))),
+                    each undirected edge stored once, oriented from the lower to
+                    the higher node id of a seeded random relabelling, like
+                    the once-per-edge storage of com-dblp; self loops and
+                    duplicates removed.
+* ``lattice3d``  -- an s^3 lattice with 6-neighbour directed edges kept with
+                    probability p plus a fraction of random long edges (the
+                    fe_body-like mesh of the SG config).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _dedup(rows: np.ndarray) -> np.ndarray:
+    if rows.size == 0:
+        return rows.reshape(0, 2).astype(np.int32)
+    key = (rows[:, 0].astype(np.int64) << 32) | (rows[:, 1].astype(np.int64) & 0xFFFFFFFF)
+    _, idx = np.unique(key, return_index=True)
+    return np.ascontiguousarray(rows[np.sort(idx)]).astype(np.int32)
+
+
+def dag(n: int = 5000, p: float = 0.7, extra: int = 2000, span: int = 64, seed: int = 0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    chain = np.nonzero(rng.random(n - 1) < p)[0]
+    e1 = np.stack([chain, chain + 1], axis=1)
+    u = rng.integers(0, n, size=extra)
+    v = u + rng.integers(1, span + 1, size=extra)
+    keep = v < n
+    e2 = np.stack([u[keep], v[keep]], axis=1)
+    return _dedup(np.concatenate([e1, e2]).astype(np.int64))
+
+
+def chung_lu(n: int = 317_000, m: int = 1_050_000, gamma: float = 2.5, orient_noise: float = 0.065,
+             seed: int = 0) -> np.ndarray:
+    """m distinct undirected edges, each stored once. An edge points from the
+    endpoint with the smaller score to the larger, score = degree rank +
+    orient_noise * n * U(0,1) (mostly hub -> leaf). At the defaults the
+    closure holds ~1.9e9 tuples (com-dblp scale). Node ids are a seeded
+    random relabelling of the ranks."""
+    rng = np.random.default_rng(seed)
+    w = np.arange(1, n + 1, dtype=np.float64) ** (-1.0 / (gamma - 1.0))
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    score = np.arange(n) + orient_noise * n * rng.random(n)
+    ids = rng.permutation(n)
+    out = np.zeros((0, 2), dtype=np.int64)
+    while out.shape[0] < m:
+        k = int((m - out.shape[0]) * 1.3) + 1024
+        a = np.searchsorted(cdf, rng.random(k))
+        b = np.searchsorted(cdf, rng.random(k))
+        ok = a != b
+        a, b = a[ok], b[ok]
+        fwd = score[a] < score[b]
+        src = np.where(fwd, a, b)
+        dst = np.where(fwd, b, a)
+        cand = np.concatenate([out, np.stack([src, dst], axis=1)])
+        key = (cand[:, 0] << 32) | cand[:, 1]
+        _, idx = np.unique(key, return_index=True)
+        out = cand[np.sort(idx)]
+    out = out[:m]
+    return np.ascontiguousarray(ids[out]).astype(np.int32)
+
+
+def lattice3d(side: int = 55, p: float = 0.15, long_frac: float = 0.01, seed: int = 0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    n = side ** 3
+    idx = np.arange(n, dtype=np.int64)
+    x, y, z = idx % side, (idx // side) % side, idx // (side * side)
+    parts = []
+    for dim, coord, step in ((0, x, 1), (1, y, side), (2, z, side * side)):
+        for sgn in (1, -1):
+            ok = (coord + sgn >= 0) & (coord + sgn < side)
+            src = idx[ok]
+            dst = src + sgn * step
+            keep = rng.random(src.size) < p
+            parts.append(np.stack([src[keep], dst[keep]], axis=1))
+    local = np.concatenate(parts)
+    nl = int(local.shape[0] * long_frac)
+    lu = rng.integers(0, n, size=nl)
+    lv = rng.integers(0, n, size=nl)
+    ok = lu != lv
+    rows = np.concatenate([local, np.stack([lu[ok], lv[ok]], axis=1)])
+    return _dedup(rows)
+
+
+CONFIGS = {
+    # name: (program, generator, kwargs)
+    "c0_tc_dag": ("tc", dag, {}),
+    "c1_tc_chung_lu": ("tc", chung_lu, {}),
+    "c2_sg_lattice": ("sg", lattice3d, {}),
+}
+
+
+def make(name: str, seed: int = 0) -> tuple[str, np.ndarray]:
+    prog, fn, kw = CONFIGS[name]
+    return prog, fn(seed=seed, **kw)

@@ -1,0 +1,113 @@
+"""Fixpoint programs on the GPU against the golden outputs and the live oracle
+(bit-exact rows in the reference's file order, iteration counts and the
+per-iteration delta sizes)."""
+import numpy as np
+import pytest
+
+from conftest import load_expected, load_input, sha_rows
+from oracle import cpu
+
+pytestmark = pytest.mark.gpu
+
+EXP = load_expected()
+CASES = [(f, p) for f, e in EXP["inputs"].items() for p in ("tc", "sg", "wcc") if p in e]
+
+
+@pytest.mark.parametrize("fname,prog", CASES)
+def test_golden(engine, fname, prog):
+    e = load_input(fname)
+    rec = EXP["inputs"][fname][prog]
+    if prog == "wcc":
+        for mode in ("reference", "fixpoint"):
+            r = engine.wcc(e, wcc_stop=mode, labels=True)
+            w = rec[mode]
+            assert (r.output_tuples, r.largest_component, r.iterations) == \
+                (w["components"], w["largest"], w["iterations"]), mode
+            assert r.deltas.tolist() == w["deltas"]
+            assert sha_rows(r.rows) == w["rows_sha256"]
+            assert sha_rows(np.stack([r.node_ids, r.labels], 1)) == w["labels_sha256"]
+    else:
+        r = engine.run(prog, e)
+        assert len(r.rows) == rec["rows_count"]
+        assert r.iterations == rec["iterations"]
+        assert r.deltas.tolist() == rec["deltas"]
+        assert sha_rows(r.rows) == rec["rows_sha256"]
+
+
+@pytest.mark.parametrize("case", EXP["single_join"], ids=lambda c: f"{c['rows']}x{c['rand_range']}")
+def test_single_join_golden(engine, case):
+    from mnmgdatalog_b200 import generate_rows
+    rows = generate_rows(case["rows"], case["rand_range"], 1)
+    assert sha_rows(rows) == case["generated_sha256"]
+    r = engine.single_join(rows)
+    assert len(r.rows) == case["rows_count"] and r.iterations == 1
+    assert sha_rows(r.rows) == case["rows_sha256"]
+
+
+def _edge_cases():
+    rng = np.random.default_rng(0)
+    yield "single_edge", np.array([[1, 2]], np.int32)
+    yield "self_loop", np.array([[5, 5]], np.int32)
+    yield "two_cycle", np.array([[1, 2], [2, 1]], np.int32)
+    yield "duplicates", np.array([[1, 2], [1, 2], [2, 3], [2, 3], [3, 1]], np.int32)
+    yield "negative_ids", np.array([[-5, -1], [-1, 3], [3, -7], [-7, -5]], np.int32)
+    yield "extreme_ids", np.array([[-2**31, 2**31 - 1], [2**31 - 1, 0], [0, -2**31]], np.int32)
+    yield "sparse_ids", (rng.integers(0, 60, (150, 2)) * 35_000_000 - 2**30).astype(np.int32)
+    yield "random_dense", rng.integers(0, 400, (1500, 2)).astype(np.int32)
+    yield "star_out", np.stack([np.zeros(3000, np.int32), np.arange(1, 3001, dtype=np.int32)], 1)
+    yield "star_in", np.stack([np.arange(1, 3001, dtype=np.int32), np.zeros(3000, np.int32)], 1)
+    yield "chain", np.stack([np.arange(0, 700), np.arange(1, 701)], 1).astype(np.int32)
+
+
+EDGE_CASES = list(_edge_cases())
+
+
+@pytest.mark.parametrize("name,e", EDGE_CASES, ids=[c[0] for c in EDGE_CASES])
+@pytest.mark.parametrize("prog", ["tc", "sg"])
+def test_against_oracle(engine, name, e, prog):
+    want = cpu.tc(e) if prog == "tc" else cpu.sg(e)
+    got = engine.run(prog, e)
+    assert np.array_equal(got.rows, want.rows)
+    assert got.iterations == want.iterations
+    assert got.deltas.tolist() == want.deltas.tolist()
+
+
+@pytest.mark.parametrize("name,e", EDGE_CASES, ids=[c[0] for c in EDGE_CASES])
+@pytest.mark.parametrize("mode", ["reference", "fixpoint"])
+def test_wcc_against_oracle(engine, name, e, mode):
+    want = cpu.wcc(e, cpu.STOP_REFERENCE if mode == "reference" else cpu.STOP_FIXPOINT)
+    got = engine.wcc(e, wcc_stop=mode, labels=True)
+    assert np.array_equal(got.rows, want.comp_rows)
+    assert (got.largest_component, got.iterations) == (want.largest, want.iterations)
+    assert got.deltas.tolist() == want.deltas.tolist()
+    assert np.array_equal(got.node_ids, want.node_ids) and np.array_equal(got.labels, want.labels)
+
+
+@pytest.mark.parametrize("prog", ["tc", "sg", "wcc", "single_join"])
+def test_empty_input(engine, prog):
+    r = engine.run(prog, np.zeros((0, 2), np.int32))
+    assert len(r.rows) == 0
+
+
+def test_device_input_matches_host_input(engine):
+    import torch
+    e = load_input("data_7035.bin")
+    a = engine.tc(e)
+    b = engine.tc(torch.from_numpy(e).cuda(), output="device")
+    assert np.array_equal(a.rows, b.rows.cpu().numpy())
+    assert a.deltas.tolist() == b.deltas.tolist()
+
+
+def test_repeated_runs_reuse_buffers(engine):
+    e = load_input("synth_dag_c0.bin")
+    first = engine.tc(e)
+    for _ in range(3):
+        r = engine.tc(e)
+        assert np.array_equal(r.rows, first.rows)
+
+
+def test_phase_timing(engine):
+    r = engine.tc(load_input("data_7035.bin"), phase_timing=True)
+    assert r.seconds > 0 and set(r.phases) == {"initialization", "join", "deduplication", "merge",
+                                               "finalization"}
+    assert sum(r.phases.values()) > 0

@@ -1,0 +1,72 @@
+"""The engine against the reference's own GPU programs (tc.cu, sg.cu, wcc.cu,
+tc_nl.cu, sg_nl.cu, single_join.cu built unmodified by oracle/Makefile and run
+as one MPI rank): byte-identical output files and the same CSV counts."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_input
+
+pytestmark = pytest.mark.gpu
+
+REF = os.path.join(ROOT, "oracle", "_ref")
+FILES = ["data_5.bin", "data_10.bin", "data_22.bin", "hipc_2019.bin", "dummy.bin", "paper.bin", "tc_paper.bin",
+         "quiz3.bin", "data_7035.bin", "data_23874.bin", "synth_dag_c0.bin", "synth_lattice_small.bin"]
+
+
+def _ref_bin(name):
+    p = os.path.join(REF, name)
+    if not os.path.exists(p):
+        pytest.skip(f"{p} not built (oracle/Makefile `make ref` needs the reference sources)")
+    return p
+
+
+def _run_ref(binary, fname, tmp_path, suffix):
+    inp = tmp_path / fname
+    load_input(fname).astype("<i4").tofile(inp)
+    out = str(inp) + suffix
+    if os.path.exists(out):
+        os.remove(out)
+    r = subprocess.run([binary, str(inp)], capture_output=True, text=True, timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    lines = [l for l in r.stdout.splitlines() if l and l[0].isdigit()]
+    csv = lines[-1].split(",")
+    rows = np.fromfile(out, dtype="<i4").reshape(-1, 2) if os.path.exists(out) else np.zeros((0, 2), np.int32)
+    return csv, rows
+
+
+@pytest.mark.parametrize("fname", FILES)
+@pytest.mark.parametrize("prog,binary,suffix", [("tc", "tc.out", "_tc.bin"), ("tc", "tc_nl.out", "_tc.bin"),
+                                                ("sg", "sg.out", "_sg.bin"), ("sg", "sg_nl.out", "_sg.bin")])
+def test_tc_sg_files_identical(engine, tmp_path, fname, prog, binary, suffix):
+    if prog == "sg" and fname == "data_23874.bin":
+        pytest.skip("SG of TG.cedge is large for the reference's int sizes")
+    csv, ref_rows = _run_ref(_ref_bin(binary), fname, tmp_path, suffix)
+    ours = engine.run(prog, load_input(fname))
+    assert int(csv[2]) == ours.iterations
+    assert int(csv[3]) == len(ours.rows)
+    assert np.array_equal(ref_rows, ours.rows)
+
+
+@pytest.mark.parametrize("fname", FILES + ["data_214078.bin", "data_223001.bin"])
+def test_wcc_file_identical(engine, tmp_path, fname):
+    csv, ref_rows = _run_ref(_ref_bin("wcc.out"), fname, tmp_path, "_cc.bin")
+    ours = engine.wcc(load_input(fname), wcc_stop="reference")
+    assert int(csv[2]) == ours.iterations
+    assert (int(csv[3]), int(csv[4])) == (ours.output_tuples, ours.largest_component)
+    assert np.array_equal(ref_rows, ours.rows)
+
+
+@pytest.mark.parametrize("rows,rand_range", [(1000, 100), (20000, 5000), (200000, 200000)])
+def test_single_join_count(engine, tmp_path, rows, rand_range):
+    from mnmgdatalog_b200 import generate_rows
+    binary = _ref_bin("single_join.out")
+    r = subprocess.run([binary, str(rows), "0", "0", str(rand_range)], capture_output=True, text=True,
+                       timeout=300, cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    csv = [l for l in r.stdout.splitlines() if l and l[0].isdigit()][-1].split(",")
+    ours = engine.single_join(generate_rows(rows, rand_range, 1))
+    assert int(csv[3]) == len(ours.rows)
