@@ -1,0 +1,356 @@
+"""Benchmark: derived tuples/s per fixpoint of the B200 Datalog engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c1_tc_chung_lu|c0_tc_dag|c2_sg_lattice]
+
+Default workload (one step = one whole TC fixpoint, init through the last
+iteration): transitive closure of a seeded Chung-Lu power-law graph with 317K
+nodes, exponent 2.5 and 1.05M edges stored once (~1.9e9 closure tuples), the
+com-dblp-scale configuration of the reference's TC results. `value` is
+closure tuples per second with the edge relation already in HBM; `e2e` is the
+same metric through the public API with host buffers (pinned H2D of the edges,
+the fixpoint, D2H of every closure row). Under torchrun every rank runs its own
+independent replica (the path is one fixpoint per GPU; no collective on the
+data path); timing is on the device (CUDA events) and the max over ranks.
+
+--impl reference times the reference's own CPU program (rough/tc_mpi.cpp, built
+by oracle/Makefile into oracle/_ref/tc_mpi; one MPI rank = one core) on a
+bounded sample of the same graph family, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "derived tuples/s per fixpoint"
+UNIT = "tuples/s"
+L2_FLUSH_BYTES = 256 << 20
+CPU_SAMPLE_NODES = 8000      # cpu_baseline sample (~15-25 s on one core)
+REF_SAMPLE_NODES = 6000      # reference arm sample per step (~5-10 s)
+HBM_FALLBACK_GBS = 6650.0
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def workload(config: str):
+    from mnmgdatalog_b200 import graphs
+    prog, edges = graphs.make(config, seed=0)
+    return prog, edges
+
+
+def describe(config: str, edges: np.ndarray) -> dict:
+    d = {"c1_tc_chung_lu": "TC, Chung-Lu n=317000 gamma=2.5 m=1050000 (each edge once, seed 0)",
+         "c0_tc_dag": "TC, DAG n=5000 p=0.7 + 2000 short edges (seed 0)",
+         "c2_sg_lattice": "SG, 55^3 lattice 6-neighbour p=0.15 + 1% long edges (seed 0)"}
+    return {"workload": d.get(config, config), "config": config, "input_rows": int(len(edges))}
+
+
+def measured_peak_gbs() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        exe = shutil.which("nvidia-smi")
+        if not exe:
+            return
+        self.proc = subprocess.Popen([exe, f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_tc_mpi_sample(nodes: int, seed: int = 0) -> dict:
+    """Time the reference CPU program on a Chung-Lu sample of `nodes` nodes."""
+    from mnmgdatalog_b200 import graphs
+    e = graphs.chung_lu(n=nodes, m=int(round(nodes * 1_050_000 / 317_000)), seed=seed)
+    binary = os.path.join(ROOT, "oracle", "_ref", "tc_mpi")
+    with tempfile.TemporaryDirectory() as td:
+        inp = os.path.join(td, "sample.bin")
+        e.astype("<i4").tofile(inp)
+        if os.path.exists(binary):
+            t0 = time.perf_counter()
+            r = subprocess.run([binary, inp], capture_output=True, text=True, timeout=600, check=True)
+            wall = time.perf_counter() - t0
+            row = [l for l in r.stdout.splitlines() if l.startswith("|") and l[2:3].isdigit()][-1]
+            cells = [c.strip().replace(",", "").replace("'", "") for c in row.strip("|").split("|")]
+            tuples, secs = int(cells[3]), float(cells[4])
+            kind = "reference"
+        else:  # the oracle's C restatement (same algorithm as the reference GPU path)
+            from oracle import cpu
+            t0 = time.perf_counter()
+            res = cpu.tc(e)
+            secs = wall = time.perf_counter() - t0
+            tuples = len(res.rows)
+            kind = "port"
+    return {"value": tuples / secs, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"TC of Chung-Lu n={nodes} m={len(e)} gamma=2.5 (same generator, seed {seed}): "
+                      f"{tuples} tuples in {secs:.2f} s (wall {wall:.2f} s), one MPI rank",
+            "tuples": tuples, "seconds": secs}
+
+
+def main_reference(args, rank: int, world: int) -> int:
+    if rank != 0:
+        return 0
+    for _ in range(args.warmup):
+        run_tc_mpi_sample(REF_SAMPLE_NODES)
+    vals, secs = [], []
+    for _ in range(args.steps):
+        r = run_tc_mpi_sample(REF_SAMPLE_NODES)
+        vals.append(r["value"])
+        secs.append(r["seconds"])
+    total_tuples = r["tuples"] * args.steps
+    value = total_tuples / sum(secs)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": r["sample"], "config": args.config, "l2": "host CPU run"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main_ours(args, rank: int, world: int, local_rank: int) -> int:
+    import torch
+    import torch.distributed as dist
+
+    from mnmgdatalog_b200 import Engine
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    prog, edges = workload(args.config)
+    stream = torch.cuda.Stream(device=dev)
+    eng = Engine(local_rank, stream=stream)
+    d_edges = torch.from_numpy(edges).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def step():
+        return eng.run(prog, d_edges, output="none")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    eng.profile(True)
+    evs = []
+    tuples = 0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)                      # L2 flush, outside the timed events
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        r = step()
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        evs.append((a, b))
+        tuples += r.output_tuples
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    prof = eng.profile_read()
+    eng.profile(False)
+    my_ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([my_ms], dtype=torch.float64, device=dev)
+    tot = torch.tensor([float(tuples)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    max_ms = float(t.item())
+    value = float(tot.item()) / (max_ms / 1e3)
+
+    # dominant kernel class by device time over the timed region
+    peak, peak_kind = measured_peak_gbs()
+    dom_name, dom = max(((k, v) for k, v in prof.items() if v["timed_launches"]), key=lambda kv: kv[1]["seconds"])
+    launches = sum(v["launches"] for v in prof.values())
+    achieved = dom["bytes"] / dom["seconds"] / 1e9 if dom["seconds"] else 0.0
+    traffic = traffic_per_launch(dom_name, dom)
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": traffic, "launches": dom["timed_launches"],
+                "share_of_step": dom["seconds"] / (my_ms / 1e3),
+                "algorithmic_bytes_per_launch": dom["bytes"] / max(dom["timed_launches"], 1)}
+    kernels = {k: {"launches": v["launches"], "ms": round(1e3 * v["seconds"], 3),
+                   "GBps": round(v["bytes"] / v["seconds"] / 1e9, 1) if v["seconds"] else None}
+               for k, v in prof.items() if v["launches"]}
+
+    e2e = None
+    if not args.no_e2e:
+        try:
+            e2e = measure_e2e(eng, prog, edges, args, dev, world, barrier)
+        except Exception as exc:  # reported in the line, never hidden
+            e2e = {"value": None, "unit": UNIT, "error": f"{type(exc).__name__}: {exc}"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = run_tc_mpi_sample(CPU_SAMPLE_NODES)
+            cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as exc:  # report, never hide
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        cfg = describe(args.config, edges)
+        cfg.update({"parallelism": f"replicas x{world}", "l2": "256 MiB write between steps (outside timing)",
+                    "output_tuples_per_step": int(r.output_tuples), "iterations": int(r.iterations),
+                    "join_rows_per_step": int(r.join_rows_total), "join_rows_max_iteration": int(r.join_rows_max)})
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clk, "kernels": kernels}
+        print(json.dumps(line))
+    eng.close()
+    return 0
+
+
+def traffic_per_launch(kernel: str, stat: dict):
+    """DRAM bytes per launch: the ncu-measured DRAM/algorithmic byte ratio of
+    this kernel class (profiles/ncu_traffic.json) times this run's
+    algorithmic bytes per launch; null without a capture."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            ratio = json.load(f)[kernel]["dram_per_algorithmic_byte"]
+    except Exception:
+        return None
+    return ratio * stat["bytes"] / max(stat["timed_launches"], 1)
+
+
+def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
+    import torch
+    import torch.distributed as dist
+    h_edges = torch.from_numpy(edges).pin_memory().numpy()
+    probe = eng.run(prog, h_edges, output="none")
+    out = torch.empty((probe.output_tuples if prog != "wcc" else 0, 2), dtype=torch.int32).pin_memory().numpy()
+    steps = max(1, min(args.steps, 3))
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    tuples = 0
+    for _ in range(steps):
+        r = eng.run(prog, h_edges, output="host", out=out)
+        tuples += r.output_tuples
+    torch.cuda.synchronize(dev)
+    sec = time.perf_counter() - t0
+    t = torch.tensor([sec], dtype=torch.float64, device=dev)
+    tot = torch.tensor([float(tuples)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    return {"value": float(tot.item()) / float(t.item()), "unit": UNIT,
+            "h2d_bytes_per_step": int(edges.nbytes), "d2h_bytes_per_step": int(probe.output_rows * 8),
+            "steps": steps, "timer": "host wall clock, synchronized"}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", default="c1_tc_chung_lu")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            return main_reference(args, rank, world)
+        return main_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -97,6 +97,8 @@ typedef struct dl_run_info {
     double seconds_dedup;
     double seconds_merge;
     double seconds_finalize;
+    int64_t join_rows_total;     /* join output rows over all iterations (before dedup) */
+    int64_t join_rows_max;       /* largest join output of one iteration */
 } dl_run_info;
 
 DL_API const char *dl_status_string(dl_status s);
@@ -179,6 +181,21 @@ DL_API dl_status dl_run_copy_deltas(const dl_run *run, int64_t *dst, int64_t cap
 /* WCC: every node id (ascending) and its final component label. */
 DL_API dl_status dl_run_copy_labels(const dl_run *run, int32_t *node_ids, int32_t *labels, int64_t capacity);
 DL_API dl_status dl_run_destroy(dl_run *run);
+
+/* ---- live kernel profile (CUDA events on the context stream) ---- */
+
+typedef struct dl_kernel_stat {
+    char name[32];          /* kernel class, e.g. "sort_onesweep_pass" */
+    int64_t launches;       /* launches since the last dl_profile_enable */
+    int64_t timed_launches; /* launches bracketed by events (profiling on) */
+    double seconds;         /* summed device time of the timed launches */
+    double bytes;           /* summed algorithmic HBM bytes of the timed launches */
+} dl_kernel_stat;
+
+/* Reset the counters; enabled = 1 also times every launch with events. */
+DL_API dl_status dl_profile_enable(dl_context *ctx, int32_t enabled);
+/* Copy up to `capacity` kernel classes; *count = number of classes. */
+DL_API dl_status dl_profile_read(dl_context *ctx, dl_kernel_stat *out, int32_t capacity, int32_t *count);
 
 /* The reference's synthetic single-join rows: C library srand(seed) then
  * rand() % rand_range + 1 for 2*rows values (glibc generator). */

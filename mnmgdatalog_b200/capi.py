@@ -30,7 +30,7 @@ EXPORTS = (
     "dl_build_hash_table", "dl_hash_table_info", "dl_hash_table_destroy", "dl_join", "dl_join_sorted",
     "dl_run_program", "dl_run_tc", "dl_run_sg", "dl_run_wcc", "dl_run_single_join",
     "dl_run_get_info", "dl_run_copy_output", "dl_run_copy_deltas", "dl_run_copy_labels", "dl_run_destroy",
-    "dl_generate_rows",
+    "dl_generate_rows", "dl_profile_enable", "dl_profile_read",
 )
 
 
@@ -50,7 +50,12 @@ class dl_run_info(C.Structure):
                 ("output_rows", C.c_int64), ("output_tuples", C.c_int64), ("largest_component", C.c_int64),
                 ("nodes", C.c_int64), ("seconds_total", C.c_double), ("seconds_init", C.c_double),
                 ("seconds_join", C.c_double), ("seconds_dedup", C.c_double), ("seconds_merge", C.c_double),
-                ("seconds_finalize", C.c_double)]
+                ("seconds_finalize", C.c_double), ("join_rows_total", C.c_int64), ("join_rows_max", C.c_int64)]
+
+
+class dl_kernel_stat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("timed_launches", C.c_int64),
+                ("seconds", C.c_double), ("bytes", C.c_double)]
 
 
 _lib = None
@@ -98,6 +103,8 @@ def lib():
         "dl_run_copy_labels": ([vp, vp, vp, i64], C.c_int),
         "dl_run_destroy": ([vp], C.c_int),
         "dl_generate_rows": ([i64, i32, C.c_uint32, vp], C.c_int),
+        "dl_profile_enable": ([vp, i32], C.c_int),
+        "dl_profile_read": ([vp, C.POINTER(dl_kernel_stat), i32, C.POINTER(C.c_int32)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

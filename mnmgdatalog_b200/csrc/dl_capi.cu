@@ -423,6 +423,33 @@ DL_API dl_status dl_run_destroy(dl_run *run) {
     return DL_OK;
 }
 
+DL_API dl_status dl_profile_enable(dl_context *ctx, int32_t enabled) {
+    DL_REQUIRE(ctx, "ctx is NULL");
+    return guarded([&] {
+        set_device(ctx);
+        ctx->c.sync();
+        ctx->c.prof_reset();
+        ctx->c.prof_on = enabled != 0;
+    });
+}
+
+DL_API dl_status dl_profile_read(dl_context *ctx, dl_kernel_stat *out, int32_t capacity, int32_t *count) {
+    DL_REQUIRE(ctx && count && capacity >= 0 && (out || capacity == 0), "invalid argument");
+    return guarded([&] {
+        set_device(ctx);
+        ctx->c.sync();
+        *count = dl::K_COUNT;
+        for (int k = 0; k < dl::K_COUNT && k < capacity; ++k) {
+            std::memset(&out[k], 0, sizeof(dl_kernel_stat));
+            std::strncpy(out[k].name, dl::kernel_name(k), sizeof(out[k].name) - 1);
+            out[k].launches = (int64_t) ctx->c.kstat[k].launches;
+            out[k].timed_launches = (int64_t) ctx->c.kstat[k].timed;
+            out[k].seconds = ctx->c.kstat[k].seconds;
+            out[k].bytes = ctx->c.kstat[k].bytes;
+        }
+    });
+}
+
 DL_API dl_status dl_generate_rows(int64_t rows, int32_t rand_range, uint32_t seed, int32_t *host_out) {
     DL_REQUIRE(rows >= 0 && rand_range > 0 && (host_out || rows == 0), "invalid argument");
     GlibcRand g(seed);

@@ -67,6 +67,9 @@ void Context::give_back(DevBuf &buf) {
 }
 
 void Context::release_all() {
+    prof_resolve();
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    ev_pool.clear();
     for (auto &s : spares) s.release();
     spares.clear();
     DevBuf *all[] = {&ws.input, &ws.ids, &ws.w0, &ws.w1, &ws.csr_off, &ws.csr_val, &ws.full[0], &ws.full[1],
@@ -106,10 +109,69 @@ void Context::check_device_error() {
     }
 }
 
+const char *kernel_name(int kid) {
+    static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_bucket_scan", "sort_onesweep_pass",
+                                         "select_compact", "join_count_scan", "join_partition", "join_emit",
+                                         "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build"};
+    return (kid >= 0 && kid < K_COUNT) ? names[kid] : "?";
+}
+
+void Context::prof_begin() {
+    if (!prof_on) return;
+    cudaEvent_t e;
+    if (ev_pool.empty()) {
+        DL_CUDA(cudaEventCreate(&e));
+    } else {
+        e = ev_pool.back();
+        ev_pool.pop_back();
+    }
+    DL_CUDA(cudaEventRecord(e, stream));
+    prof_open = e;
+}
+
+void Context::prof_end(int kid, double bytes) {
+    kstat[kid].launches++;
+    if (!prof_on || !prof_open) return;
+    cudaEvent_t e;
+    if (ev_pool.empty()) {
+        DL_CUDA(cudaEventCreate(&e));
+    } else {
+        e = ev_pool.back();
+        ev_pool.pop_back();
+    }
+    DL_CUDA(cudaEventRecord(e, stream));
+    pending.push_back({kid, prof_open, e, bytes});
+    prof_open = nullptr;
+}
+
+void Context::prof_add_bytes(int kid, double bytes) {
+    if (prof_on) kstat[kid].bytes += bytes;
+}
+
+void Context::prof_resolve() {
+    for (auto &p : pending) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            kstat[p.kid].seconds += ms * 1e-3;
+            kstat[p.kid].timed++;
+            kstat[p.kid].bytes += p.bytes;
+        }
+        ev_pool.push_back(p.a);
+        ev_pool.push_back(p.b);
+    }
+    pending.clear();
+}
+
+void Context::prof_reset() {
+    prof_resolve();
+    for (auto &k : kstat) k = KernelStat();
+}
+
 void Context::sync() {
     DL_CUDA(cudaMemcpyAsync(reinterpret_cast<u32 *>(host_scalars) + 2 * 63, &ctrl->err, sizeof(u32),
                             cudaMemcpyDeviceToHost, stream));
     DL_CUDA(cudaStreamSynchronize(stream));
+    if (!pending.empty()) prof_resolve();
     check_device_error();
 }
 

@@ -208,13 +208,11 @@ void rank_nodes(Context &ctx, const int32_t *rows, u64 n, Graph &g) {
     const u64 m = 2 * n;
     ctx.reserve(ws.w0, m * 8);
     ctx.reserve(ws.w1, m * 8);
-    ids_to_words_kernel<<<grid_for(m, T256, ctx), T256, 0, ctx.stream>>>(rows, m, ws.w0.as<u64>());
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_PREP, 0, ids_to_words_kernel<<<grid_for(m, T256, ctx), T256, 0, ctx.stream>>>(rows, m, ws.w0.as<u64>()));
     u64 *s = radix_sort(ctx, ws.w0.as<u64>(), ws.w1.as<u64>(), m, Codec::Raw, 32);
     const u64 nu = unique_words(ctx, s, m, s);
     ctx.reserve(ws.ids, nu * 4);
-    words_to_ids_kernel<<<grid_for(nu, T256, ctx), T256, 0, ctx.stream>>>(s, nu, ws.ids.as<int32_t>());
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_PREP, 0, words_to_ids_kernel<<<grid_for(nu, T256, ctx), T256, 0, ctx.stream>>>(s, nu, ws.ids.as<int32_t>()));
     g.n_ids = (u32) nu;
     g.bits = bits_for(nu);
     g.ids = ws.ids.as<int32_t>();
@@ -225,13 +223,11 @@ void build_csr(Context &ctx, const u64 *words, u64 n, Graph &g) {
     Workspace &ws = ctx.ws;
     ctx.reserve(ws.csr_off, ((u64) g.n_ids + 1) * 4);
     ctx.reserve(ws.csr_val, std::max<u64>(n, 1) * 4);
-    csr_offsets_kernel<<<grid_for((u64) g.n_ids + 1, T256, ctx), T256, 0, ctx.stream>>>(words, n, g.bits, g.n_ids,
-                                                                                         ws.csr_off.as<u32>());
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_PREP, 0, csr_offsets_kernel<<<grid_for((u64) g.n_ids + 1, T256, ctx), T256, 0, ctx.stream>>>(words, n, g.bits, g.n_ids,
+                                                                                         ws.csr_off.as<u32>()));
     if (n) {
-        csr_values_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(words, n, (1ull << g.bits) - 1,
-                                                                          ws.csr_val.as<u32>());
-        DL_CHECK_LAUNCH();
+        DL_LAUNCH(ctx, K_PREP, 0, csr_values_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(words, n, (1ull << g.bits) - 1,
+                                                                          ws.csr_val.as<u32>()));
     }
     g.csr.off = ws.csr_off.as<u32>();
     g.csr.val = ws.csr_val.as<u32>();
@@ -262,6 +258,8 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
     ctx.reserve(ws.offsets, std::max<u64>(n_probe, 1) * 8);
     const u64 total = join_count(ctx, g.csr, probe, n_probe, g.bits, ws.offsets.as<u64>());
     n_j = total;
+    ctx.run_join_total += total;
+    ctx.run_join_max = std::max(ctx.run_join_max, total);
     DevBuf &jout = other(ws, probe);
     ctx.reserve(jout, std::max<u64>(total, 1) * 8);
     if (total == 0) return jout.as<u64>();
@@ -279,6 +277,8 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
 }
 
 void finish_info(Run &r, Context &ctx, cudaEvent_t e0, cudaEvent_t e1, PhaseTimer &pt) {
+    r.info.join_rows_total = (i64) ctx.run_join_total;
+    r.info.join_rows_max = (i64) ctx.run_join_max;
     DL_CUDA(cudaEventSynchronize(e1));
     float ms = 0;
     DL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
@@ -334,9 +334,8 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         rank_nodes(ctx, rows, n, g);
         ctx.reserve(ws.jbuf[0], n * 8);
         ctx.reserve(ws.jbuf[1], n * 8);
-        pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
-                                                                         ws.w0.as<u64>(), ws.jbuf[0].as<u64>());
-        DL_CHECK_LAUNCH();
+        DL_LAUNCH(ctx, K_PREP, 0, pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
+                                                                         ws.w0.as<u64>(), ws.jbuf[0].as<u64>()));
         u64 ne;
         u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, n, 2 * g.bits, ne);
         build_csr(ctx, e, ne, g);
@@ -396,9 +395,8 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         rank_nodes(ctx, rows, n, g);
         ctx.reserve(ws.jbuf[0], n * 8);
         ctx.reserve(ws.jbuf[1], n * 8);
-        pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
-                                                                         ws.jbuf[0].as<u64>(), nullptr);
-        DL_CHECK_LAUNCH();
+        DL_LAUNCH(ctx, K_PREP, 0, pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
+                                                                         ws.jbuf[0].as<u64>(), nullptr));
         u64 ne;
         u64 *e = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * g.bits, ne);  // sg.cu:150-153
         build_csr(ctx, e, ne, g);                                                    // sg.cu:162
@@ -468,8 +466,7 @@ static void run_wcc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, bo
         ctx.reserve(ws.jbuf[0], 2 * n * 8);
         ctx.reserve(ws.jbuf[1], 2 * n * 8);
         u64 *w = ws.jbuf[0].as<u64>();
-        pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits, w, w + n);
-        DL_CHECK_LAUNCH();
+        DL_LAUNCH(ctx, K_PREP, 0, pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits, w, w + n));
         u64 ne;
         u64 *e = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], 2 * n, 2 * g.bits, ne);  // wcc.cu:140-167
         build_csr(ctx, e, ne, g);
@@ -481,7 +478,7 @@ static void run_wcc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, bo
         ctx.reserve(ws.w1, (u64) nn * 8);
         u32 *label = ws.wcc_label.as<u32>(), *flag = ws.wcc_flag.as<u32>(), *next = ws.wcc_next.as<u32>();
         u64 *dcur = ws.w0.as<u64>(), *dnext = ws.w1.as<u64>();
-        wcc_init_kernel<<<grid_for(nn, T256, ctx), T256, 0, ctx.stream>>>(nn, label, flag, dcur);  // wcc.cu:211-231
+        DL_LAUNCH(ctx, K_PREP, 0, wcc_init_kernel<<<grid_for(nn, T256, ctx), T256, 0, ctx.stream>>>(nn, label, flag, dcur));  // wcc.cu:211-231
         DL_CHECK_LAUNCH();
         u32 *next_count = reinterpret_cast<u32 *>(&ctx.ctrl->scalar[9]);
         u64 ndelta = nn;
@@ -492,14 +489,15 @@ static void run_wcc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, bo
             DL_CUDA(cudaMemsetAsync(next_count, 0, sizeof(u32), ctx.stream));
             WccSrc src{g.csr.off, g.csr.val, dcur, label, flag, next, next_count};
             const u64 total = count_matches(ctx, src, ndelta, ws.offsets.as<u64>());
+            ctx.run_join_total += total;
+            ctx.run_join_max = std::max(ctx.run_join_max, total);
             if (total) emit_matches(ctx, src, ndelta, ws.offsets.as<u64>(), total, nullptr, nullptr, 0, nullptr);
             pt.mark(PH_MERGE);
             DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 2, next_count, sizeof(u32), cudaMemcpyDeviceToHost, ctx.stream));
             ctx.sync();
             const u64 nnew = *reinterpret_cast<u32 *>(ctx.host_scalars + 2);
             if (nnew) {
-                wcc_next_delta_kernel<<<grid_for(nnew, T256, ctx), T256, 0, ctx.stream>>>(next, nnew, label, flag, dnext);
-                DL_CHECK_LAUNCH();
+                DL_LAUNCH(ctx, K_PREP, 0, wcc_next_delta_kernel<<<grid_for(nnew, T256, ctx), T256, 0, ctx.stream>>>(next, nnew, label, flag, dnext));
             }
             std::swap(dcur, dnext);
             ndelta = nnew;
@@ -516,16 +514,14 @@ static void run_wcc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, bo
         pt.mark(PH_FINAL);
         u32 *cnt = reinterpret_cast<u32 *>(ws.w1.p);  // reuse: nn u32 counters
         DL_CUDA(cudaMemsetAsync(cnt, 0, (u64) nn * 4, ctx.stream));
-        wcc_count_kernel<<<grid_for(nn, T256, ctx), T256, 0, ctx.stream>>>(label, nn, cnt);
-        DL_CHECK_LAUNCH();
+        DL_LAUNCH(ctx, K_PREP, 0, wcc_count_kernel<<<grid_for(nn, T256, ctx), T256, 0, ctx.stream>>>(label, nn, cnt));
         u64 *pos = ws.w0.as<u64>();
         u64 *largest = &ctx.ctrl->scalar[10];
         DL_CUDA(cudaMemsetAsync(largest, 0, sizeof(u64), ctx.stream));
         const u64 ncomp = count_matches(ctx, NonZeroCounter{cnt}, nn, pos);
         ctx.reserve(r.aux, std::max<u64>(ncomp, 1) * 4);
-        wcc_components_kernel<<<grid_for(nn, T256, ctx), T256, 0, ctx.stream>>>(
-            cnt, nn, pos, r.aux.as<u32>(), reinterpret_cast<unsigned long long *>(largest));
-        DL_CHECK_LAUNCH();
+        DL_LAUNCH(ctx, K_PREP, 0, wcc_components_kernel<<<grid_for(nn, T256, ctx), T256, 0, ctx.stream>>>(
+            cnt, nn, pos, r.aux.as<u32>(), reinterpret_cast<unsigned long long *>(largest)));
         DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 3, largest, sizeof(u64), cudaMemcpyDeviceToHost, ctx.stream));
         ctx.sync();
         r.n_aux = ncomp;
@@ -557,9 +553,8 @@ static void run_single_join_impl(Context &ctx, Run &r, const int32_t *rows_in, u
         rank_nodes(ctx, rows, n, g);
         ctx.reserve(ws.jbuf[0], n * 8);
         ctx.reserve(ws.jbuf[1], n * 8);
-        pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
-                                                                         ws.w0.as<u64>(), ws.jbuf[0].as<u64>());
-        DL_CHECK_LAUNCH();
+        DL_LAUNCH(ctx, K_PREP, 0, pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
+                                                                         ws.w0.as<u64>(), ws.jbuf[0].as<u64>()));
         u64 ne, np;
         u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, n, 2 * g.bits, ne);  // single_join.cu:165-168
         build_csr(ctx, e, ne, g);
@@ -586,6 +581,7 @@ Run *run_program(Context &ctx, int program, const int32_t *rows, u64 n, bool on_
     r->program = (dl_program) program;
     r->info.program = program;
     r->info.input_rows = (i64) n;
+    ctx.run_join_total = ctx.run_join_max = 0;
     try {
         switch (program) {
             case DL_PROGRAM_TC: run_tc_impl(ctx, *r, rows, n, on_device, opt); break;
@@ -615,12 +611,12 @@ void run_copy_output(const Run &r, int32_t *dst, u64 capacity, bool dst_on_devic
     }
     const int32_t *ids = r.ids.as<int32_t>();
     if (r.program == DL_PROGRAM_WCC) {
-        unpack_components_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.aux.as<u32>(), n, ids, tmp);
+        DL_LAUNCH(ctx, K_PREP, 0, unpack_components_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.aux.as<u32>(), n, ids, tmp));
     } else if (r.program == DL_PROGRAM_SG) {
-        unpack_rows_kernel<true><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.words.as<u64>(), n, r.bits, ids, tmp);
+        DL_LAUNCH(ctx, K_PREP, 0, unpack_rows_kernel<true><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.words.as<u64>(), n, r.bits, ids, tmp));
     } else {
-        unpack_rows_kernel<false><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.words.as<u64>(), n, r.bits, ids,
-                                                                                   tmp);
+        DL_LAUNCH(ctx, K_PREP, 0, unpack_rows_kernel<false><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.words.as<u64>(), n, r.bits, ids,
+                                                                                   tmp));
     }
     DL_CHECK_LAUNCH();
     if (!dst_on_device) DL_CUDA(cudaMemcpyAsync(dst, tmp, n * 8, cudaMemcpyDeviceToHost, ctx.stream));
@@ -636,9 +632,8 @@ void run_copy_labels(const Run &r, int32_t *node_ids, int32_t *labels, u64 capac
     if (n == 0) return;
     DevBuf stage;
     ctx.reserve(stage, n * 4);
-    unpack_labels_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.labels.as<u32>(), (u32) n,
-                                                                         r.ids.as<int32_t>(), stage.as<int32_t>());
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_PREP, 0, unpack_labels_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.labels.as<u32>(), (u32) n,
+                                                                         r.ids.as<int32_t>(), stage.as<int32_t>()));
     DL_CUDA(cudaMemcpyAsync(labels, stage.p, n * 4, cudaMemcpyDeviceToHost, ctx.stream));
     DL_CUDA(cudaMemcpyAsync(node_ids, r.ids.p, n * 4, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();

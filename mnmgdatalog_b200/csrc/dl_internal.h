@@ -33,6 +33,16 @@ struct Error : std::runtime_error {
 
 #define DL_CHECK_LAUNCH() DL_CUDA(cudaGetLastError())
 
+// Brackets one kernel launch for the live profile:
+//   DL_LAUNCH(ctx, K_SORT_PASS, 16.0 * n, kernel<<<g, b, s, ctx.stream>>>(...));
+#define DL_LAUNCH(ctx, kid, bytes, ...)   \
+    do {                                  \
+        (ctx).prof_begin();               \
+        __VA_ARGS__;                      \
+        DL_CHECK_LAUNCH();                \
+        (ctx).prof_end((kid), (bytes));   \
+    } while (0)
+
 // Grow-only device buffer; no allocation happens inside a fixpoint iteration
 // once the capacities have reached their high-water mark.
 struct DevBuf {
@@ -42,6 +52,33 @@ struct DevBuf {
     void release();
     template <typename T>
     T *as() const { return static_cast<T *>(p); }
+};
+
+// Kernel classes for the live profile (launch counts, device time from CUDA
+// events on the context stream, algorithmic HBM bytes).
+enum KernelId : int {
+    K_PREP = 0,        // init / finalize transforms (pack, rank, CSR, unpack)
+    K_SORT_HIST,       // radix histogram pass
+    K_SORT_BUCKET,     // radix bucket scan
+    K_SORT_PASS,       // onesweep radix pass: 16 B per key
+    K_SELECT,          // unique / remove_if compaction: 8 B read + 8 B per kept word
+    K_JOIN_COUNT,      // join count + scan: 8 B probe read + 8 B offset write per probe row
+    K_JOIN_PARTITION,  // merge-path partition of the emit
+    K_JOIN_EMIT,       // join emit: 8 B per probe row + 16 B per output word
+    K_WCC_PROPAGATE,   // WCC min-label propagation: 8 B per delta row + 4 B per edge + 32 B per atomicMin
+    K_MERGE_PARTITION, // merge-path partition of set operations
+    K_DIFF_MERGE,      // fused unique/set-difference/merge: 8 B x (|full| + |J| + |full'| + |delta|)
+    K_MERGE,           // plain merge: 16 B per word
+    K_HASH_BUILD,      // C-ABI hash table insert / value extraction
+    K_COUNT
+};
+const char *kernel_name(int kid);
+
+struct KernelStat {
+    u64 launches = 0;
+    u64 timed = 0;
+    double seconds = 0;
+    double bytes = 0;
 };
 
 // Engine scratch reused across runs of one context (capacities only grow).
@@ -68,7 +105,26 @@ struct Context {
     DevBuf lbs_splits;              // join emit partition points
     u64 *host_scalars = nullptr;    // pinned mirror for small D2H reads
     Workspace ws;
+    u64 run_join_total = 0, run_join_max = 0;  // join statistics of the current run
     std::vector<DevBuf> spares;     // buffers handed back by destroyed runs
+
+    // Live profile: every launch is counted; with prof_on each launch is
+    // bracketed by events that are resolved at the next sync().
+    bool prof_on = false;
+    KernelStat kstat[K_COUNT];
+    struct Pending {
+        int kid;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> ev_pool;
+    cudaEvent_t prof_open = nullptr;
+    void prof_begin();
+    void prof_end(int kid, double bytes);
+    void prof_add_bytes(int kid, double bytes);
+    void prof_resolve();
+    void prof_reset();
 
     // Ensure buf holds `bytes`, preferring a spare buffer over cudaMalloc.
     void reserve(DevBuf &buf, size_t bytes, bool zero = false);

@@ -110,11 +110,9 @@ HashTable *hash_table_build(Context &ctx, const u64 *rel, u64 n, double load_fac
         ht->table.reserve(slots * sizeof(HashSlot), true);
         ht->vals.reserve(n * sizeof(u32));
         const unsigned grid = (unsigned) std::min<u64>((n + 255) / 256, (u64) ctx.sm_count * 16);
-        hash_insert_kernel<<<grid, 256, 0, ctx.stream>>>(sorted, n, ht->table.as<HashSlot>(), slots - 1,
-                                                         &ctx.ctrl->err);
-        DL_CHECK_LAUNCH();
-        extract_values_kernel<<<grid, 256, 0, ctx.stream>>>(sorted, n, ht->vals.as<u32>());
-        DL_CHECK_LAUNCH();
+        DL_LAUNCH(ctx, K_HASH_BUILD, 8.0 * n, hash_insert_kernel<<<grid, 256, 0, ctx.stream>>>(sorted, n, ht->table.as<HashSlot>(), slots - 1,
+                                                         &ctx.ctrl->err));
+        DL_LAUNCH(ctx, K_HASH_BUILD, 8.0 * n, extract_values_kernel<<<grid, 256, 0, ctx.stream>>>(sorted, n, ht->vals.as<u32>()));
         ctx.sync();
     } catch (...) {
         a.release();

@@ -26,6 +26,8 @@ struct CsrSrc {
     int bits;
     static constexpr bool kSelfFilter = (K == EmitKind::ZV_NOSELF);
     static constexpr bool kWrite = true;
+    static constexpr int kProfKind = K_JOIN_EMIT;
+    static double prof_bytes(u64 n, u64 total) { return 8.0 * n + 16.0 * total; }
     __device__ __forceinline__ u64 degree(u64 i) const {
         const u32 k = (u32) (probe[i] >> bits);
         return (u64) (off[k + 1] - off[k]);
@@ -67,6 +69,8 @@ struct HashSrc {
     const u64 *probe;
     static constexpr bool kSelfFilter = false;
     static constexpr bool kWrite = true;
+    static constexpr int kProfKind = K_JOIN_EMIT;
+    static double prof_bytes(u64 n, u64 total) { return 8.0 * n + 16.0 * total; }
     __device__ __forceinline__ void lookup(u32 key, u64 &begin, u64 &count) const {
         u64 h = fmix32(key) & mask;
         for (u64 step = 0; step <= mask; ++step) {
@@ -103,6 +107,8 @@ struct SortedSrc {
     const u64 *probe;
     static constexpr bool kSelfFilter = false;
     static constexpr bool kWrite = true;
+    static constexpr int kProfKind = K_JOIN_EMIT;
+    static double prof_bytes(u64 n, u64 total) { return 8.0 * n + 16.0 * total; }
     __device__ __forceinline__ u64 bound(int key, bool upper) const {
         u64 lo = 0, hi = n_rel;
         while (lo < hi) {
@@ -141,6 +147,8 @@ struct WccSrc {
     u32 *next_count;
     static constexpr bool kSelfFilter = false;
     static constexpr bool kWrite = false;
+    static constexpr int kProfKind = K_WCC_PROPAGATE;
+    static double prof_bytes(u64 n, u64 total) { return 8.0 * n + 36.0 * total; }
     __device__ __forceinline__ u64 degree(u64 i) const {
         const u32 k = (u32) (delta[i] >> 32);
         return (u64) (off[k + 1] - off[k]);
@@ -252,9 +260,8 @@ u64 count_matches(Context &ctx, const Src &src, u64 n, u64 *offsets) {
     u32 *ctr = ctx.tile_counter(48);
     u64 *tot = &ctx.ctrl->scalar[2];
     DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(u32), ctx.stream));
-    scan_kernel<DegreeOp<Src>><<<(unsigned) tiles, SCAN_THREADS, 0, ctx.stream>>>(
-        DegreeOp<Src>{src}, n, offsets, lb, ctr, ctx.next_epoch(), &ctx.ctrl->err, tot);
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_JOIN_COUNT, 16.0 * n, scan_kernel<DegreeOp<Src>><<<(unsigned) tiles, SCAN_THREADS, 0, ctx.stream>>>(
+        DegreeOp<Src>{src}, n, offsets, lb, ctr, ctx.next_epoch(), &ctx.ctrl->err, tot));
     DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, tot, sizeof(u64), cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
     return ctx.host_scalars[0];
@@ -267,14 +274,12 @@ void emit_matches(Context &ctx, const Src &src, u64 n, const u64 *offsets, u64 t
     const u64 tiles = (n + total + JN_TILE - 1) / JN_TILE;
     ctx.lbs_splits.reserve((tiles + 1) * sizeof(u64));
     u64 *splits = ctx.lbs_splits.as<u64>();
-    lbs_partition_kernel<<<(unsigned) ((tiles + 1 + 255) / 256), 256, 0, ctx.stream>>>(offsets, n, total, tiles + 1,
-                                                                                     splits);
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_JOIN_PARTITION, 0, lbs_partition_kernel<<<(unsigned) ((tiles + 1 + 255) / 256), 256, 0, ctx.stream>>>(offsets, n, total, tiles + 1,
+                                                                                     splits));
     auto kern = join_emit_kernel<Src>;
     DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(JoinSmem)));
-    kern<<<(unsigned) tiles, JN_THREADS, sizeof(JoinSmem), ctx.stream>>>(src, n, offsets, total, splits, out, hist,
-                                                                         ndig, self_pairs);
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, Src::kProfKind, Src::prof_bytes(n, total), kern<<<(unsigned) tiles, JN_THREADS, sizeof(JoinSmem), ctx.stream>>>(src, n, offsets, total, splits, out, hist,
+                                                                         ndig, self_pairs));
 }
 
 HashTable *hash_table_build(Context &ctx, const u64 *rel, u64 n, double load_factor);

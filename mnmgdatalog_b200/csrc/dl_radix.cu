@@ -166,16 +166,11 @@ onesweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int sh
 template <bool ENC, bool DEC>
 void launch_onesweep(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, const u64 *bucket, u64 *lb,
                      u32 *ctr) {
-    static bool configured = false;
     auto kern = onesweep_kernel<ENC, DEC>;
-    if (!configured) {
-        DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(SortSmem)));
-        configured = true;
-    }
+    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(SortSmem)));
     const u64 tiles = (n + SORT_TILE - 1) / SORT_TILE;
-    kern<<<(unsigned) tiles, SORT_THREADS, sizeof(SortSmem), ctx.stream>>>(in, out, n, shift, bucket, lb, ctr,
-                                                                          ctx.next_epoch(), &ctx.ctrl->err);
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_SORT_PASS, 16.0 * n, kern<<<(unsigned) tiles, SORT_THREADS, sizeof(SortSmem), ctx.stream>>>(in, out, n, shift, bucket, lb, ctr,
+                                                                          ctx.next_epoch(), &ctx.ctrl->err));
 }
 
 }  // namespace
@@ -206,13 +201,11 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
     if (!hist_accumulated) {
         radix_hist_clear(ctx);
         if (ent)
-            radix_hist_kernel<true><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist);
+            DL_LAUNCH(ctx, K_SORT_HIST, 8.0 * n, radix_hist_kernel<true><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist));
         else
-            radix_hist_kernel<false><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist);
-        DL_CHECK_LAUNCH();
+            DL_LAUNCH(ctx, K_SORT_HIST, 8.0 * n, radix_hist_kernel<false><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist));
     }
-    radix_bucket_kernel<<<ndig, RADIX, 0, ctx.stream>>>(hist, bucket, n, mask);
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_SORT_BUCKET, 0, radix_bucket_kernel<<<ndig, RADIX, 0, ctx.stream>>>(hist, bucket, n, mask));
     if (known_bits > 0 && !ent) {
         for (int d = 0; d < ndig; ++d) digits[nd++] = d;
     } else {

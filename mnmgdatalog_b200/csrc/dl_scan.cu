@@ -27,11 +27,11 @@ u64 run_select(Context &ctx, const u64 *in, u64 n, u64 *out, Keep keep) {
     u32 *ctr = ctx.tile_counter(32);
     u64 *cnt = &ctx.ctrl->scalar[0];
     DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(u32), ctx.stream));
-    select_kernel<Keep><<<(unsigned) tiles, SCAN_THREADS, 0, ctx.stream>>>(in, n, out, keep, lb, ctr,
-                                                                          ctx.next_epoch(), &ctx.ctrl->err, cnt);
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_SELECT, 8.0 * n, select_kernel<Keep><<<(unsigned) tiles, SCAN_THREADS, 0, ctx.stream>>>(in, n, out, keep, lb, ctr,
+                                                                          ctx.next_epoch(), &ctx.ctrl->err, cnt));
     DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, cnt, sizeof(u64), cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
+    ctx.prof_add_bytes(K_SELECT, 8.0 * ctx.host_scalars[0]);
     return ctx.host_scalars[0];
 }
 

@@ -206,9 +206,8 @@ u64 *partition(Context &ctx, const u64 *a, u64 na, const u64 *b, u64 nb, Codec c
     // look-back buffer; the split points follow them.
     u64 *splits = ctx.lookback_words(2 * (tiles + 1)) + (tiles + 1);
     const unsigned grid = (unsigned) ((tiles + 1 + 255) / 256);
-    if (codec == Codec::Entity) merge_partition_kernel<true><<<grid, 256, 0, ctx.stream>>>(a, na, b, nb, tiles + 1, splits);
-    else merge_partition_kernel<false><<<grid, 256, 0, ctx.stream>>>(a, na, b, nb, tiles + 1, splits);
-    DL_CHECK_LAUNCH();
+    if (codec == Codec::Entity) DL_LAUNCH(ctx, K_MERGE_PARTITION, 0, merge_partition_kernel<true><<<grid, 256, 0, ctx.stream>>>(a, na, b, nb, tiles + 1, splits));
+    else DL_LAUNCH(ctx, K_MERGE_PARTITION, 0, merge_partition_kernel<false><<<grid, 256, 0, ctx.stream>>>(a, na, b, nb, tiles + 1, splits));
     return splits;
 }
 
@@ -217,9 +216,8 @@ void launch_diff_merge(Context &ctx, const u64 *full, u64 nfull, const u64 *j, u
                        u64 *full_out, u64 *delta_out, u64 *lb, u32 *ctr, u64 *cnt) {
     auto kern = diff_merge_kernel<ENC, WF, WD>;
     DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(MpSmem)));
-    kern<<<(unsigned) tiles, MP_THREADS, sizeof(MpSmem), ctx.stream>>>(full, nfull, j, nj, splits, full_out, delta_out,
-                                                                       lb, ctr, ctx.next_epoch(), &ctx.ctrl->err, cnt);
-    DL_CHECK_LAUNCH();
+    DL_LAUNCH(ctx, K_DIFF_MERGE, 8.0 * (2 * nfull + nj), kern<<<(unsigned) tiles, MP_THREADS, sizeof(MpSmem), ctx.stream>>>(full, nfull, j, nj, splits, full_out, delta_out,
+                                                                       lb, ctr, ctx.next_epoch(), &ctx.ctrl->err, cnt));
 }
 
 }  // namespace
@@ -230,10 +228,10 @@ void merge_words(Context &ctx, const u64 *a, u64 na, const u64 *b, u64 nb, u64 *
     u64 *splits = partition(ctx, a, na, b, nb, codec, tiles);
     if (codec == Codec::Entity) {
         DL_CUDA(cudaFuncSetAttribute(merge_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(MpSmem)));
-        merge_kernel<true><<<(unsigned) tiles, MP_THREADS, sizeof(MpSmem), ctx.stream>>>(a, na, b, nb, splits, out);
+        DL_LAUNCH(ctx, K_MERGE, 16.0 * (na + nb), merge_kernel<true><<<(unsigned) tiles, MP_THREADS, sizeof(MpSmem), ctx.stream>>>(a, na, b, nb, splits, out));
     } else {
         DL_CUDA(cudaFuncSetAttribute(merge_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(MpSmem)));
-        merge_kernel<false><<<(unsigned) tiles, MP_THREADS, sizeof(MpSmem), ctx.stream>>>(a, na, b, nb, splits, out);
+        DL_LAUNCH(ctx, K_MERGE, 16.0 * (na + nb), merge_kernel<false><<<(unsigned) tiles, MP_THREADS, sizeof(MpSmem), ctx.stream>>>(a, na, b, nb, splits, out));
     }
     DL_CHECK_LAUNCH();
 }
@@ -262,7 +260,9 @@ u64 diff_merge_words(Context &ctx, const u64 *full, u64 nfull, const u64 *j, u64
 #undef DL_DM
     DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, cnt, sizeof(u64), cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
-    return ctx.host_scalars[0];
+    const u64 nd = ctx.host_scalars[0];
+    ctx.prof_add_bytes(K_DIFF_MERGE, 8.0 * ((wf ? (double) nd : -(double) nfull) + (wd ? (double) nd : 0.0)));
+    return nd;
 }
 
 }  // namespace dl

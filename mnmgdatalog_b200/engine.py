@@ -48,6 +48,8 @@ class RunResult:
     seconds: float               # device time of the run (input upload through last iteration)
     phases: dict = field(default_factory=dict)
     largest_component: int = 0   # WCC
+    join_rows_total: int = 0     # join output rows over all iterations (before dedup)
+    join_rows_max: int = 0
     node_ids: np.ndarray | None = None
     labels: np.ndarray | None = None
 
@@ -126,12 +128,26 @@ class Engine:
     def synchronize(self):
         check(lib().dl_context_synchronize(self.ctx))
 
+    def profile(self, enabled: bool = True) -> None:
+        """Reset the live kernel profile; enabled=True times every launch."""
+        check(lib().dl_profile_enable(self.ctx, 1 if enabled else 0))
+
+    def profile_read(self) -> dict:
+        """{kernel class: {launches, timed_launches, seconds, bytes}}."""
+        arr = (capi.dl_kernel_stat * 64)()
+        n = C.c_int32()
+        check(lib().dl_profile_read(self.ctx, arr, 64, C.byref(n)))
+        return {arr[i].name.decode(): {"launches": arr[i].launches, "timed_launches": arr[i].timed_launches,
+                                       "seconds": arr[i].seconds, "bytes": arr[i].bytes}
+                for i in range(min(n.value, 64))}
+
     # ---- programs ----------------------------------------------------------
     def run(self, program: str, edges, *, wcc_stop: str = "reference", max_iterations: int = 0,
-            phase_timing: bool = False, output: str = "host", labels: bool = False) -> RunResult:
+            phase_timing: bool = False, output: str = "host", labels: bool = False, out=None) -> RunResult:
         """Run one program. `edges` is an (n, 2) int32 host array or a CUDA
         tensor (then the input stays on the device). `output` is "host"
-        (numpy), "device" (torch tensor) or "none"."""
+        (numpy), "device" (torch tensor) or "none"; `out` optionally supplies
+        the (capacity, 2) int32 destination (e.g. pinned host memory)."""
         torch = _torch()
         prog = PROGRAMS[program]
         opts = capi.dl_options()
@@ -140,7 +156,7 @@ class Engine:
         opts.phase_timing = 1 if phase_timing else 0
         keep = None
         if isinstance(edges, torch.Tensor) and edges.is_cuda:
-            keep = _check_rel(edges)
+            keep = _check_rel(edges) if edges.numel() else edges
             ptr, n, on_dev = keep.data_ptr(), keep.shape[0] if keep.numel() else 0, 1
         else:
             keep = _as_rows_np(edges)
@@ -155,13 +171,20 @@ class Engine:
             nout = info.output_rows
             rows = None
             if output == "host":
-                rows = np.empty((nout, 2), dtype=np.int32)
+                if out is not None:
+                    if len(out) < nout or out.dtype != np.int32 or not out.flags.c_contiguous:
+                        raise DatalogError(1, f"out holds {len(out)} rows, the result has {nout}")
+                    rows = out[:nout]
+                else:
+                    rows = np.empty((nout, 2), dtype=np.int32)
                 check(lib().dl_run_copy_output(run, rows.ctypes.data if nout else None, nout, 0))
             elif output == "device":
-                rows = torch.empty((nout, 2), dtype=torch.int32, device=f"cuda:{self.device}")
+                rows = out[:nout] if out is not None else torch.empty((nout, 2), dtype=torch.int32,
+                                                                      device=f"cuda:{self.device}")
                 check(lib().dl_run_copy_output(run, C.c_void_p(rows.data_ptr()) if nout else None, nout, 1))
             res = RunResult(program, rows, info.iterations, deltas, info.output_tuples, info.nodes,
-                            info.seconds_total, largest_component=info.largest_component)
+                            info.seconds_total, largest_component=info.largest_component,
+                            join_rows_total=info.join_rows_total, join_rows_max=info.join_rows_max)
             if phase_timing:
                 res.phases = {"initialization": info.seconds_init, "join": info.seconds_join,
                               "deduplication": info.seconds_dedup, "merge": info.seconds_merge,
