@@ -299,7 +299,8 @@ def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
     import torch.distributed as dist
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
     probe = eng.run(prog, h_edges, output="none")
-    out = torch.empty((probe.output_tuples if prog != "wcc" else 0, 2), dtype=torch.int32).pin_memory().numpy()
+    out_rows = probe.output_tuples
+    out = torch.empty((out_rows, 2), dtype=torch.int32).pin_memory().numpy()
     steps = max(1, min(args.steps, 3))
     barrier()
     torch.cuda.synchronize(dev)
@@ -316,7 +317,7 @@ def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.all_reduce(tot, op=dist.ReduceOp.SUM)
     return {"value": float(tot.item()) / float(t.item()), "unit": UNIT,
-            "h2d_bytes_per_step": int(edges.nbytes), "d2h_bytes_per_step": int(probe.output_rows * 8),
+            "h2d_bytes_per_step": int(edges.nbytes), "d2h_bytes_per_step": int(out_rows * 8),
             "steps": steps, "timer": "host wall clock, synchronized"}
 
 

@@ -139,27 +139,99 @@ __device__ __forceinline__ u64 lookback_warp(const u64 *lb, u32 tile, u32 epoch,
     }
 }
 
-// Serial look-back of one counter column (used per radix digit): word for
-// tile t lives at lb[t * stride].
+// Block-wide decoupled look-back: every thread reads one predecessor's word,
+// so one round covers NWARPS*32 tiles -- more than the tiles resident on the
+// GPU at a time -- and a tile typically finds an inclusive prefix in one L2
+// round trip (a warp-wide window lags the inclusive frontier by many rounds
+// when tiles are short). All threads of the block must call it.
+struct LookbackScratch {
+    u32 first_inc;
+    u32 bad;
+    u64 part[32];
+};
+
+template <int NWARPS>
+__device__ __forceinline__ u64 lookback_block(const u64 *lb, u32 tile, u32 epoch, u32 *err, LookbackScratch &sc) {
+    constexpr int NT = NWARPS * 32;
+    const int tid = threadIdx.x;
+    u64 excl = 0;
+    long long base = (long long) tile - 1;
+    u32 spins = 0;
+    while (true) {
+        const long long t = base - tid;
+        const u64 w = (t >= 0) ? ld_relaxed_u64(lb + t) : (kStatusInc | ((u64) (epoch & kEpochMask) << 48));
+        u32 st = (u32) (w >> 62);
+        if (((u32) (w >> 48) & kEpochMask) != (epoch & kEpochMask)) st = 0;
+        if (tid == 0) {
+            sc.first_inc = NT;
+            sc.bad = 0;
+        }
+        __syncthreads();
+        if (st == 2) atomicMin(&sc.first_inc, (u32) tid);
+        __syncthreads();
+        const u32 fi = sc.first_inc;
+        if (st == 0 && (u32) tid <= fi) sc.bad = 1;
+        __syncthreads();
+        if (sc.bad) {
+            ++spins;
+            if (spins > kSpinLimit) {
+                if (tid == 0) atomicOr(err, DL_DEVERR_LOOKBACK);
+                __syncthreads();
+                return excl;
+            }
+            if (spins > 64) __nanosleep(64);
+            __syncthreads();  // every thread has read sc.bad before it is reset
+            continue;
+        }
+        u64 v = ((u32) tid <= fi) ? (w & kLbValueMask) : 0ull;
+        v = warp_sum(v);
+        if (lane_id() == 0) sc.part[tid >> 5] = v;
+        __syncthreads();
+        u64 sum = 0;
+#pragma unroll
+        for (int i = 0; i < NWARPS; ++i) sum += sc.part[i];
+        excl += sum;
+        __syncthreads();  // part[] and first_inc read before the next round
+        if (fi < (u32) NT) return excl;
+        base -= NT;
+    }
+}
+
+// Look-back of one counter column (used per radix digit): the word of tile t
+// lives at lb[t * stride]. Reads a window of 8 predecessors per round.
 __device__ __forceinline__ u64 lookback_serial(const u64 *lb, u32 tile, u32 stride, u32 epoch, u32 *err) {
+    constexpr int WIN = 8;
     u64 excl = 0;
     long long t = (long long) tile - 1;
     u32 spins = 0;
     while (t >= 0) {
-        u64 w = ld_relaxed_u64(lb + (u64) t * stride);
-        u32 st = (u32) (w >> 62);
-        if (((u32) (w >> 48) & kEpochMask) != (epoch & kEpochMask)) st = 0;
-        if (st == 0) {
+        u64 w[WIN];
+#pragma unroll
+        for (int i = 0; i < WIN; ++i) w[i] = (t - i >= 0) ? ld_relaxed_u64(lb + (u64) (t - i) * stride) : 0ull;
+        int consumed = 0;
+        bool done = false, stall = false;
+#pragma unroll
+        for (int i = 0; i < WIN; ++i) {
+            if (done || stall || t - i < 0) continue;
+            u32 st = (u32) (w[i] >> 62);
+            if (((u32) (w[i] >> 48) & kEpochMask) != (epoch & kEpochMask)) st = 0;
+            if (st == 0) {
+                stall = true;
+                continue;
+            }
+            excl += w[i] & kLbValueMask;
+            ++consumed;
+            if (st == 2) done = true;
+        }
+        if (done) return excl;
+        t -= consumed;
+        if (stall) {
             if (++spins > kSpinLimit) {
                 atomicOr(err, DL_DEVERR_LOOKBACK);
                 return excl;
             }
             if (spins > 32) __nanosleep(32);
-            continue;
         }
-        excl += w & kLbValueMask;
-        if (st == 2) break;
-        --t;
     }
     return excl;
 }

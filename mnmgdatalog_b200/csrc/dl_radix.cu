@@ -27,6 +27,7 @@ constexpr int HIST_THREADS = 512;
 struct SortSmem {
     u64 keys[SORT_TILE];
     u32 warp_cnt[SORT_WARPS][RADIX];
+    u32 match[SORT_WARPS][RADIX];  // peer masks of the atomicOr ranking
     u64 gbase[RADIX];
     u32 tile_start[RADIX];
     u32 scratch[SORT_WARPS + 1];
@@ -67,7 +68,14 @@ __global__ void __launch_bounds__(RADIX) radix_bucket_kernel(const u64 *__restri
     if (c == n) atomicOr(trivial_mask, 1u << d);
 }
 
-template <bool ENC, bool DEC>
+// Ranking of a key's digit among the warp's lanes ("peers"):
+//   RANK_BALLOT = 0: 8 warp ballots, one per digit bit;
+//   RANK_ATOMIC = 1: every lane sets its bit in a per-(warp, digit) shared
+//                    mask with atomicOr and reads the mask back.
+constexpr int RANK_BALLOT = 0;
+constexpr int RANK_ATOMIC = 1;
+
+template <bool ENC, bool DEC, int RANK>
 __global__ void __launch_bounds__(SORT_THREADS, 2)
 onesweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int shift,
                 const u64 *__restrict__ bucket, u64 *lb, u32 *tile_ctr, u32 epoch, u32 *err) {
@@ -77,7 +85,10 @@ onesweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int sh
     const u32 lane = tid & 31;
     const int w = tid >> 5;
 
-    for (int i = tid; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&s.warp_cnt[0][0])[i] = 0;
+    for (int i = tid; i < SORT_WARPS * RADIX; i += SORT_THREADS) {
+        (&s.warp_cnt[0][0])[i] = 0;
+        if (RANK == RANK_ATOMIC) (&s.match[0][0])[i] = 0;
+    }
     if (tid == 0) s.tile = atomicAdd(tile_ctr, 1u);
     __syncthreads();
     const u32 tile = s.tile;
@@ -104,18 +115,27 @@ onesweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int sh
 #pragma unroll
     for (int i = 0; i < SORT_KPT; ++i) {
         const u32 d = (u32) (k[i] >> shift) & 255u;
-        u32 peers = 0xffffffffu;
+        u32 peers;
+        if (RANK == RANK_BALLOT) {
+            peers = 0xffffffffu;
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const u32 bit = (d >> b) & 1u;
-            const u32 bal = __ballot_sync(0xffffffffu, bit);
-            peers &= bit ? bal : ~bal;
+            for (int b = 0; b < 8; ++b) {
+                const u32 bit = (d >> b) & 1u;
+                const u32 bal = __ballot_sync(0xffffffffu, bit);
+                peers &= bit ? bal : ~bal;
+            }
+        } else {
+            atomicOr(&s.match[w][d], 1u << lane);
+            __syncwarp();
+            peers = *reinterpret_cast<volatile u32 *>(&s.match[w][d]);
+            __syncwarp();
         }
         const u32 leader = __ffs(peers) - 1;
         u32 prev = 0;
         if (lane == leader) {
             prev = s.warp_cnt[w][d];
             s.warp_cnt[w][d] = prev + __popc(peers);
+            if (RANK == RANK_ATOMIC) s.match[w][d] = 0;
         }
         __syncwarp();
         prev = __shfl_sync(0xffffffffu, prev, leader);
@@ -163,10 +183,21 @@ onesweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int sh
     }
 }
 
+// Ranking variant: DL_SORT_RANK=ballot|atomic (default atomic), read once.
+int rank_mode() {
+    static int mode = -1;
+    if (mode < 0) {
+        const char *e = getenv("DL_SORT_RANK");
+        mode = (e && std::string(e) == "ballot") ? RANK_BALLOT : RANK_ATOMIC;
+    }
+    return mode;
+}
+
 template <bool ENC, bool DEC>
 void launch_onesweep(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, const u64 *bucket, u64 *lb,
                      u32 *ctr) {
-    auto kern = onesweep_kernel<ENC, DEC>;
+    auto kern = rank_mode() == RANK_BALLOT ? onesweep_kernel<ENC, DEC, RANK_BALLOT>
+                                           : onesweep_kernel<ENC, DEC, RANK_ATOMIC>;
     DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(SortSmem)));
     const u64 tiles = (n + SORT_TILE - 1) / SORT_TILE;
     DL_LAUNCH(ctx, K_SORT_PASS, 16.0 * n, kern<<<(unsigned) tiles, SORT_THREADS, sizeof(SortSmem), ctx.stream>>>(in, out, n, shift, bucket, lb, ctr,

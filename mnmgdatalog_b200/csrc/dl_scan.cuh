@@ -24,6 +24,7 @@ select_kernel(const u64 *in, u64 n, u64 *out, Keep keep, u64 *lb, u32 *tile_ctr,
     __shared__ u32 s_scratch[SCAN_THREADS / 32 + 1];
     __shared__ u32 s_tile;
     __shared__ u64 s_excl;
+    __shared__ LookbackScratch s_lbs;
     const int tid = threadIdx.x;
     if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
     __syncthreads();
@@ -51,13 +52,13 @@ select_kernel(const u64 *in, u64 n, u64 *out, Keep keep, u64 *lb, u32 *tile_ctr,
     }
     u32 tot;
     const u32 off = block_exclusive_sum<SCAN_THREADS / 32>((u32) __popc(flags), s_scratch, &tot);
-    if (tid < 32) {
+    {
         u64 excl = 0;
         if (tile == 0) {
             if (tid == 0) st_relaxed_u64(lb, lb_word(kStatusInc, epoch, tot));
         } else {
             if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusAgg, epoch, tot));
-            excl = lookback_warp(lb, tile, epoch, err);
+            excl = lookback_block<SCAN_THREADS / 32>(lb, tile, epoch, err, s_lbs);
             if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusInc, epoch, excl + tot));
         }
         if (tid == 0) s_excl = excl;
@@ -87,6 +88,7 @@ scan_kernel(Value value, u64 n, u64 *out, u64 *lb, u32 *tile_ctr, u32 epoch, u32
     __shared__ u64 s_items[SCAN_TILE];
     __shared__ u32 s_tile;
     __shared__ u64 s_excl;
+    __shared__ LookbackScratch s_lbs;
     const int tid = threadIdx.x;
     if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
     __syncthreads();
@@ -108,13 +110,13 @@ scan_kernel(Value value, u64 n, u64 *out, u64 *lb, u32 *tile_ctr, u32 epoch, u32
     }
     u64 tot;
     u64 off = block_exclusive_sum<SCAN_THREADS / 32>(sum, s_scratch, &tot);
-    if (tid < 32) {
+    {
         u64 excl = 0;
         if (tile == 0) {
             if (tid == 0) st_relaxed_u64(lb, lb_word(kStatusInc, epoch, tot));
         } else {
             if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusAgg, epoch, tot));
-            excl = lookback_warp(lb, tile, epoch, err);
+            excl = lookback_block<SCAN_THREADS / 32>(lb, tile, epoch, err, s_lbs);
             if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusInc, epoch, excl + tot));
         }
         if (tid == 0) s_excl = excl;

@@ -13,15 +13,16 @@
 //
 // Each CTA takes 4096 consecutive positions of the merged order; its start in
 // both inputs comes from a partition kernel (one merge-path binary search per
-// tile boundary). Inputs are staged in shared memory, every thread merges 16
-// words serially, outputs leave through shared memory in coalesced runs.
+// tile boundary). Inputs are staged in shared memory, every thread merges 8
+// words serially, outputs leave through the same 32 KiB buffer in coalesced
+// runs (3 CTAs of 16 warps per SM).
 #include "dl_internal.h"
 
 namespace dl {
 namespace {
 
-constexpr int MP_THREADS = 256;
-constexpr int MP_VT = 16;
+constexpr int MP_THREADS = 512;
+constexpr int MP_VT = 8;
 constexpr int MP_TILE = MP_THREADS * MP_VT;
 
 template <bool ENC>
@@ -63,28 +64,59 @@ __global__ void merge_partition_kernel(const u64 *a, u64 na, const u64 *b, u64 n
     splits[t] = merge_path<ENC>(a, na, b, nb, diag);
 }
 
+// One 32 KiB buffer: the tile's inputs, then (after the merge, values in
+// registers) the staged outputs.
 struct MpSmem {
-    u64 in[MP_TILE];
-    u64 out[MP_TILE];
+    u64 buf[MP_TILE];
     u32 scratch[MP_THREADS / 32 + 1];
     u32 tile;
     u64 excl;
 };
 
-// Loads the tile's slices of a and b into s.in ([0, la) then [la, la+lb)).
+// Loads the tile's slices of a and b into s.buf ([0, la) then [la, la+lb)).
 template <bool ENC>
 __device__ __forceinline__ void load_tile(MpSmem &s, const u64 *a, u64 a0, u32 la, const u64 *b, u64 b0, u32 lb) {
-    for (u32 i = threadIdx.x; i < la + lb; i += MP_THREADS)
-        s.in[i] = (i < la) ? ld_enc<ENC>(a + a0 + i) : ld_enc<ENC>(b + b0 + (i - la));
+#pragma unroll
+    for (int k = 0; k < MP_VT; ++k) {
+        const u32 i = k * MP_THREADS + threadIdx.x;
+        if (i < la + lb) s.buf[i] = (i < la) ? ld_enc<ENC>(a + a0 + i) : ld_enc<ENC>(b + b0 + (i - la));
+    }
 }
 
+// Shared memory of diff_merge: the tile's slice of full (a), a staging
+// buffer (first the slice of J, then the full' output), and the insertion
+// index of every new J word.
+struct DmSmem {
+    u64 a[MP_TILE];
+    u64 stage[MP_TILE];
+    uint16_t ins[MP_TILE];
+    u32 scratch[MP_THREADS / 32 + 1];
+    u32 tile;
+    LookbackScratch lbs;
+};
+
+// Number of entries of the sorted list ins[lo, n) that are <= x.
+__device__ __forceinline__ u32 upper_in(const uint16_t *ins, u32 lo, u32 n, u32 x) {
+    u32 hi = n;
+    while (lo < hi) {
+        const u32 mid = (lo + hi) >> 1;
+        if (ins[mid] <= x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Shift-copy form of the fused step: only J words are searched (binary
+// search of the tile's full slice); a full word's output position is its
+// index plus the number of new J words inserted before it, so full words
+// are moved without per-word merge logic.
 template <bool ENC, bool WRITE_FULL, bool WRITE_DELTA>
-__global__ void __launch_bounds__(MP_THREADS)
+__global__ void __launch_bounds__(MP_THREADS, 3)
 diff_merge_kernel(const u64 *__restrict__ full, u64 nfull, const u64 *__restrict__ jw, u64 nj,
                   const u64 *__restrict__ splits, u64 *__restrict__ full_out, u64 *__restrict__ delta_out,
                   u64 *lb, u32 *tile_ctr, u32 epoch, u32 *err, u64 *delta_count) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MpSmem &s = *reinterpret_cast<MpSmem *>(smem_raw);
+    DmSmem &s = *reinterpret_cast<DmSmem *>(smem_raw);
     const int tid = threadIdx.x;
     if (tid == 0) s.tile = atomicAdd(tile_ctr, 1u);
     __syncthreads();
@@ -95,81 +127,103 @@ diff_merge_kernel(const u64 *__restrict__ full, u64 nfull, const u64 *__restrict
     const u64 a0 = splits[tile], a1 = splits[tile + 1];
     const u64 b0 = d0 - a0, b1 = d1 - a1;
     const u32 la = (u32) (a1 - a0), lbn = (u32) (b1 - b0);
-    load_tile<ENC>(s, full, a0, la, jw, b0, lbn);
-    __syncthreads();
-
-    const u64 *sa = s.in;
-    const u64 *sb = s.in + la;
-    const u32 td = min((u32) tid * MP_VT, la + lbn);
-    u32 ta = merge_path_smem(sa, la, sb, lbn, td);
-    u32 tb = td - ta;
-    bool hp = false;
-    u64 prev = 0;
-    if (ta > 0) { prev = sa[ta - 1]; hp = true; }
-    else if (a0 > 0) { prev = ld_enc<ENC>(full + a0 - 1); hp = true; }
-    if (tb > 0) { const u64 v = sb[tb - 1]; prev = hp ? max(prev, v) : v; hp = true; }
-    else if (b0 > 0) { const u64 v = ld_enc<ENC>(jw + b0 - 1); prev = hp ? max(prev, v) : v; hp = true; }
-
-    const u32 ta_start = ta;
-    u64 val[MP_VT];
-    u32 is_a = 0, is_new = 0;
 #pragma unroll
     for (int k = 0; k < MP_VT; ++k) {
-        val[k] = 0;
-        if (ta + tb < la + lbn) {
-            const bool take_a = ta < la && (tb >= lbn || sa[ta] <= sb[tb]);
-            const u64 v = take_a ? sa[ta] : sb[tb];
-            if (take_a) { ++ta; is_a |= 1u << k; }
-            else {
-                ++tb;
-                if (!hp || v != prev) is_new |= 1u << k;
+        const u32 i = k * MP_THREADS + tid;
+        if (i < la) s.a[i] = ld_enc<ENC>(full + a0 + i);
+        if (i < lbn) s.stage[i] = ld_enc<ENC>(jw + b0 + i);
+    }
+    __syncthreads();
+
+    // J words: blocked, MP_VT consecutive words per thread.
+    const u32 jb = (u32) tid * MP_VT;
+    u64 bv[MP_VT];
+    uint16_t bp[MP_VT];
+    u32 is_new = 0;
+    {
+        u64 prev = 0;
+        bool hp = false;
+        if (jb > 0 && jb <= lbn) { prev = s.stage[jb - 1]; hp = true; }
+        else if (jb == 0 && b0 > 0) { prev = ld_enc<ENC>(jw + b0 - 1); hp = true; }
+        const bool has_a_before = a0 > 0;
+        const u64 a_before = has_a_before ? ld_enc<ENC>(full + a0 - 1) : 0ull;
+        u32 lo = 0;
+#pragma unroll
+        for (int k = 0; k < MP_VT; ++k) {
+            bv[k] = 0;
+            bp[k] = 0;
+            if (jb + k < lbn) {
+                const u64 b = s.stage[jb + k];
+                u32 l = lo, h = la;  // lower bound of b in a[lo, la)
+                while (l < h) {
+                    const u32 mid = (l + h) >> 1;
+                    if (s.a[mid] < b) l = mid + 1;
+                    else h = mid;
+                }
+                lo = l;
+                const bool dup_a = (l < la && s.a[l] == b) || (l == 0 && has_a_before && a_before == b);
+                const bool dup_b = hp && prev == b;
+                if (!dup_a && !dup_b) is_new |= 1u << k;
+                bv[k] = b;
+                bp[k] = (uint16_t) l;
+                prev = b;
+                hp = true;
             }
-            prev = v;
-            hp = true;
-            val[k] = v;
         }
     }
     u32 tile_new;
     const u32 new_before = block_exclusive_sum<MP_THREADS / 32>((u32) __popc(is_new), s.scratch, &tile_new);
-    if (tid < 32) {
-        u64 excl = 0;
-        if (tile == 0) {
-            if (tid == 0) st_relaxed_u64(lb, lb_word(kStatusInc, epoch, tile_new));
-        } else {
-            if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusAgg, epoch, tile_new));
-            excl = lookback_warp(lb, tile, epoch, err);
-            if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusInc, epoch, excl + tile_new));
-        }
-        if (tid == 0) s.excl = excl;
+    u64 excl = 0;
+    if (tile == 0) {
+        if (tid == 0) st_relaxed_u64(lb, lb_word(kStatusInc, epoch, tile_new));
+    } else {
+        if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusAgg, epoch, tile_new));
+        excl = lookback_block<MP_THREADS / 32>(lb, tile, epoch, err, s.lbs);
+        if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusInc, epoch, excl + tile_new));
     }
-    __syncthreads();  // inputs no longer read; s.excl published
+    __syncthreads();  // J slice in s.stage no longer read
     {
-        u32 na_run = ta_start, nn_run = new_before;
+        u32 r = new_before;
 #pragma unroll
         for (int k = 0; k < MP_VT; ++k) {
-            const bool a = (is_a >> k) & 1u, nw = (is_new >> k) & 1u;
-            if (WRITE_FULL && (a || nw)) s.out[na_run + nn_run] = val[k];
-            if (WRITE_DELTA && nw) s.in[nn_run] = val[k];
-            na_run += a;
-            nn_run += nw;
+            if ((is_new >> k) & 1u) {
+                s.ins[r] = bp[k];
+                if (WRITE_FULL) s.stage[bp[k] + r] = bv[k];
+                ++r;
+            }
         }
     }
     __syncthreads();
-    const u64 excl = s.excl;
     if (WRITE_FULL) {
+        // full words, striped: position = index + new J words inserted at or before it
+        const u32 lane = tid & 31;
+        u32 c = 0;
+        for (u32 base = (tid & ~31u); base < la; base += MP_THREADS) {
+            const u32 i = base + lane;
+            c = upper_in(s.ins, c, tile_new, base);  // warp-uniform start
+            u32 ci = c;
+            while (ci < tile_new && s.ins[ci] <= i) ++ci;
+            if (i < la) s.stage[i + ci] = s.a[i];
+        }
+        __syncthreads();
         const u32 nout = la + tile_new;
         u64 *dst = full_out + a0 + excl;
-        for (u32 i = tid; i < nout; i += MP_THREADS) dst[i] = ENC ? entity_decode(s.out[i]) : s.out[i];
+        for (u32 i = tid; i < nout; i += MP_THREADS) dst[i] = ENC ? entity_decode(s.stage[i]) : s.stage[i];
     }
     if (WRITE_DELTA) {
+        u32 r = new_before;
+#pragma unroll
+        for (int k = 0; k < MP_VT; ++k)
+            if ((is_new >> k) & 1u) s.a[r++] = bv[k];  // a slice consumed above
+        __syncthreads();
         u64 *dst = delta_out + excl;
-        for (u32 i = tid; i < tile_new; i += MP_THREADS) dst[i] = ENC ? entity_decode(s.in[i]) : s.in[i];
+        for (u32 i = tid; i < tile_new; i += MP_THREADS) dst[i] = ENC ? entity_decode(s.a[i]) : s.a[i];
     }
     if (d1 == total && tid == 0) *delta_count = excl + tile_new;
 }
 
 template <bool ENC>
-__global__ void __launch_bounds__(MP_THREADS)
+__global__ void __launch_bounds__(MP_THREADS, 3)
 merge_kernel(const u64 *__restrict__ a, u64 na, const u64 *__restrict__ b, u64 nb, const u64 *__restrict__ splits,
              u64 *__restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -184,20 +238,25 @@ merge_kernel(const u64 *__restrict__ a, u64 na, const u64 *__restrict__ b, u64 n
     const u32 la = (u32) (a1 - a0), lbn = (u32) (b1 - b0);
     load_tile<ENC>(s, a, a0, la, b, b0, lbn);
     __syncthreads();
-    const u64 *sa = s.in;
-    const u64 *sb = s.in + la;
+    const u64 *sa = s.buf;
+    const u64 *sb = s.buf + la;
     const u32 td = min((u32) tid * MP_VT, la + lbn);
     u32 ta = merge_path_smem(sa, la, sb, lbn, td);
     u32 tb = td - ta;
+    u64 val[MP_VT];
 #pragma unroll
     for (int k = 0; k < MP_VT; ++k) {
         if (ta + tb < la + lbn) {
             const bool take_a = ta < la && (tb >= lbn || sa[ta] <= sb[tb]);
-            s.out[td + k] = take_a ? sa[ta++] : sb[tb++];
+            val[k] = take_a ? sa[ta++] : sb[tb++];
         }
     }
     __syncthreads();
-    for (u32 i = tid; i < la + lbn; i += MP_THREADS) out[d0 + i] = ENC ? entity_decode(s.out[i]) : s.out[i];
+#pragma unroll
+    for (int k = 0; k < MP_VT; ++k)
+        if (td + k < la + lbn) s.buf[td + k] = val[k];
+    __syncthreads();
+    for (u32 i = tid; i < la + lbn; i += MP_THREADS) out[d0 + i] = ENC ? entity_decode(s.buf[i]) : s.buf[i];
 }
 
 u64 *partition(Context &ctx, const u64 *a, u64 na, const u64 *b, u64 nb, Codec codec, u64 &tiles) {
@@ -215,8 +274,8 @@ template <bool ENC, bool WF, bool WD>
 void launch_diff_merge(Context &ctx, const u64 *full, u64 nfull, const u64 *j, u64 nj, const u64 *splits, u64 tiles,
                        u64 *full_out, u64 *delta_out, u64 *lb, u32 *ctr, u64 *cnt) {
     auto kern = diff_merge_kernel<ENC, WF, WD>;
-    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(MpSmem)));
-    DL_LAUNCH(ctx, K_DIFF_MERGE, 8.0 * (2 * nfull + nj), kern<<<(unsigned) tiles, MP_THREADS, sizeof(MpSmem), ctx.stream>>>(full, nfull, j, nj, splits, full_out, delta_out,
+    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(DmSmem)));
+    DL_LAUNCH(ctx, K_DIFF_MERGE, 8.0 * (2 * nfull + nj), kern<<<(unsigned) tiles, MP_THREADS, sizeof(DmSmem), ctx.stream>>>(full, nfull, j, nj, splits, full_out, delta_out,
                                                                        lb, ctr, ctx.next_epoch(), &ctx.ctrl->err, cnt));
 }
 
