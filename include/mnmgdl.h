@@ -178,6 +178,10 @@ DL_API dl_status dl_run_copy_output(const dl_run *run, int32_t *dst, int64_t cap
                                     int32_t dst_on_device);
 /* |delta| after each iteration (length = iterations). */
 DL_API dl_status dl_run_copy_deltas(const dl_run *run, int64_t *dst, int64_t capacity);
+/* Per iteration: join output rows (before dedup) and the size of the full
+ * relation after the iteration (TC/SG; WCC: number of labelled nodes). */
+DL_API dl_status dl_run_copy_iteration_stats(const dl_run *run, int64_t *join_rows, int64_t *full_rows,
+                                             int64_t capacity);
 /* WCC: every node id (ascending) and its final component label. */
 DL_API dl_status dl_run_copy_labels(const dl_run *run, int32_t *node_ids, int32_t *labels, int64_t capacity);
 DL_API dl_status dl_run_destroy(dl_run *run);

@@ -30,6 +30,7 @@ EXPORTS = (
     "dl_build_hash_table", "dl_hash_table_info", "dl_hash_table_destroy", "dl_join", "dl_join_sorted",
     "dl_run_program", "dl_run_tc", "dl_run_sg", "dl_run_wcc", "dl_run_single_join",
     "dl_run_get_info", "dl_run_copy_output", "dl_run_copy_deltas", "dl_run_copy_labels", "dl_run_destroy",
+    "dl_run_copy_iteration_stats",
     "dl_generate_rows", "dl_profile_enable", "dl_profile_read",
 )
 
@@ -101,6 +102,7 @@ def lib():
         "dl_run_copy_output": ([vp, vp, i64, i32], C.c_int),
         "dl_run_copy_deltas": ([vp, vp, i64], C.c_int),
         "dl_run_copy_labels": ([vp, vp, vp, i64], C.c_int),
+        "dl_run_copy_iteration_stats": ([vp, vp, vp, i64], C.c_int),
         "dl_run_destroy": ([vp], C.c_int),
         "dl_generate_rows": ([i64, i32, C.c_uint32, vp], C.c_int),
         "dl_profile_enable": ([vp, i32], C.c_int),

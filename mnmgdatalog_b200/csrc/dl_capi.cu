@@ -405,6 +405,17 @@ DL_API dl_status dl_run_copy_deltas(const dl_run *run, int64_t *dst, int64_t cap
     return DL_OK;
 }
 
+DL_API dl_status dl_run_copy_iteration_stats(const dl_run *run, int64_t *join_rows, int64_t *full_rows,
+                                             int64_t capacity) {
+    DL_REQUIRE(run && run->r && capacity >= 0, "invalid argument");
+    const auto &j = run->r->joins;
+    const auto &f = run->r->fulls;
+    DL_REQUIRE((int64_t) j.size() <= capacity, "capacity smaller than the iteration count");
+    if (join_rows && !j.empty()) std::memcpy(join_rows, j.data(), j.size() * sizeof(int64_t));
+    if (full_rows && !f.empty()) std::memcpy(full_rows, f.data(), f.size() * sizeof(int64_t));
+    return DL_OK;
+}
+
 DL_API dl_status dl_run_copy_labels(const dl_run *run, int32_t *node_ids, int32_t *labels, int64_t capacity) {
     DL_REQUIRE(run && run->r && capacity >= 0, "invalid argument");
     return guarded([&] {

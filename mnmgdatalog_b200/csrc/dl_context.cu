@@ -73,6 +73,7 @@ void Context::release_all() {
     for (auto &s : spares) s.release();
     spares.clear();
     DevBuf *all[] = {&ws.input, &ws.ids, &ws.w0, &ws.w1, &ws.csr_off, &ws.csr_val, &ws.full[0], &ws.full[1],
+                     &ws.small[0], &ws.small[1], &ws.sample,
                      &ws.jbuf[0], &ws.jbuf[1], &ws.offsets, &ws.wcc_label, &ws.wcc_flag, &ws.wcc_next,
                      &lookback, &sort_hist, &lbs_splits};
     for (DevBuf *b : all) b->release();
@@ -112,7 +113,8 @@ void Context::check_device_error() {
 const char *kernel_name(int kid) {
     static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_bucket_scan", "sort_onesweep_pass",
                                          "select_compact", "join_count_scan", "join_partition", "join_emit",
-                                         "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build"};
+                                         "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build",
+                                         "sparse_diff"};
     return (kid >= 0 && kid < K_COUNT) ? names[kid] : "?";
 }
 

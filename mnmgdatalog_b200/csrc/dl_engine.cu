@@ -315,6 +315,97 @@ void adopt_ids(Context &ctx, Run &r, const Graph &g) {
     r.info.nodes = g.n_ids;
 }
 
+// The full relation of TC/SG as two disjoint sorted duplicate-free runs: a
+// large one (ws.full[cur]) and a small one (ws.small[scur]). The reference
+// keeps one sorted array and re-merges it with every delta (tc.cu:260-286),
+// which costs O(|full|) per iteration even when the delta is tiny; here a
+// sparse join output is checked against the large run by binary probes and
+// only the small run is rewritten, and the small run is merged into the large
+// one when it reaches 1/4 of it. The iteration's delta is the same set.
+struct FullSet {
+    int cur = 0;
+    u64 nbig = 0;
+    int scur = 0;
+    u64 nsmall = 0;
+    u64 ns = 0;
+    bool sample_ok = false;
+};
+
+// Measured on B200: a binary probe costs ~50 ps per J word, the fused
+// streaming step ~13 ps per word of (large run + J), so probing wins while
+// |J| is below ~1/3 of the large run; the small run is folded into the large
+// one only once it reaches 1/4 of it (otherwise at the end).
+constexpr u64 kDenseRatio = 4;   // J is dense when |J| * 4 >= |large run|
+constexpr u64 kSmallRatio = 4;   // merge when |small run| * 4 >= |large run|
+
+// Sorted J (in one of ws.jbuf) -> delta (returned, in one of ws.jbuf);
+// updates the full relation. Returns |delta| in n_delta.
+u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta) {
+    Workspace &ws = ctx.ws;
+    n_delta = 0;
+    if (nj == 0) return j;
+    const bool dense = nj * kDenseRatio >= F.nbig;
+    DevBuf &d1buf = other(ws, j);
+    if (F.nsmall == 0 && dense) {
+        // fused: delta and the new large run in one pass
+        ctx.reserve(ws.full[1 - F.cur], (F.nbig + nj) * 8);
+        const u64 n = diff_merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, j, nj, ws.full[1 - F.cur].as<u64>(),
+                                       d1buf.as<u64>(), Codec::Raw);
+        if (n) {
+            F.cur = 1 - F.cur;
+            F.nbig += n;
+            F.sample_ok = false;
+        }
+        n_delta = n;
+        return d1buf.as<u64>();
+    }
+    // delta' = dedup(J) \ large run
+    u64 nd1;
+    if (dense) {
+        nd1 = diff_merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, j, nj, nullptr, d1buf.as<u64>(), Codec::Raw);
+    } else {
+        if (!F.sample_ok) {
+            run_sample(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.sample, F.ns);
+            F.sample_ok = true;
+        }
+        nd1 = sparse_diff_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.sample.as<u64>(), F.ns, j, nj,
+                                d1buf.as<u64>());
+    }
+    if (nd1 == 0) return j;
+    // delta = delta' \ small run; small run' = small run u delta
+    DevBuf &jb = holder(ws, j);  // J is consumed: receives delta
+    ctx.reserve(ws.small[1 - F.scur], (F.nsmall + nd1) * 8);
+    const u64 n = diff_merge_words(ctx, ws.small[F.scur].as<u64>(), F.nsmall, d1buf.as<u64>(), nd1,
+                                   ws.small[1 - F.scur].as<u64>(), jb.as<u64>(), Codec::Raw);
+    if (n) {
+        F.scur = 1 - F.scur;
+        F.nsmall += n;
+    }
+    n_delta = n;
+    if (F.nsmall && F.nsmall * kSmallRatio >= F.nbig) {
+        ctx.reserve(ws.full[1 - F.cur], (F.nbig + F.nsmall) * 8);
+        merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.small[F.scur].as<u64>(), F.nsmall,
+                    ws.full[1 - F.cur].as<u64>(), Codec::Raw);
+        F.cur = 1 - F.cur;
+        F.nbig += F.nsmall;
+        F.nsmall = 0;
+        F.sample_ok = false;
+    }
+    return jb.as<u64>();
+}
+
+// Final full relation as one sorted run in ws.full[F.cur].
+void settle(Context &ctx, FullSet &F) {
+    Workspace &ws = ctx.ws;
+    if (F.nsmall == 0) return;
+    ctx.reserve(ws.full[1 - F.cur], (F.nbig + F.nsmall) * 8);
+    merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.small[F.scur].as<u64>(), F.nsmall,
+                ws.full[1 - F.cur].as<u64>(), Codec::Raw);
+    F.cur = 1 - F.cur;
+    F.nbig += F.nsmall;
+    F.nsmall = 0;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -330,6 +421,7 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     Graph g;
     u64 nfull = 0;
     int cur = 0;
+    FullSet F;
     if (n > 0) {
         rank_nodes(ctx, rows, n, g);
         ctx.reserve(ws.jbuf[0], n * 8);
@@ -343,7 +435,8 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         u64 *d = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * g.bits, nd);  // tc.cu:178-181
         ctx.reserve(ws.full[0], nd * 8);
         DL_CUDA(cudaMemcpyAsync(ws.full[0].p, d, nd * 8, cudaMemcpyDeviceToDevice, ctx.stream));  // tc.cu:188-189
-        nfull = nd;
+        F.cur = 0;
+        F.nbig = nd;
         u64 *delta = d;
         u64 ndelta = nd;
         for (int it = 0;; ++it) {  // tc.cu:216-314
@@ -351,22 +444,17 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
             u64 *j = join_and_sort(ctx, g, delta, ndelta, EmitKind::ZV, nj, nullptr, pt);
             pt.mark(PH_MERGE);
             u64 nnew = 0;
-            if (nj > 0) {
-                ctx.reserve(ws.full[1 - cur], (nfull + nj) * 8);
-                DevBuf &dout = other(ws, j);
-                nnew = diff_merge_words(ctx, ws.full[cur].as<u64>(), nfull, j, nj, ws.full[1 - cur].as<u64>(),
-                                        dout.as<u64>(), Codec::Raw);
-                delta = dout.as<u64>();
-                if (nnew) {
-                    cur = 1 - cur;
-                    nfull += nnew;
-                }
-            }
+            delta = absorb(ctx, F, j, nj, nnew);
             ndelta = nnew;
             r.deltas.push_back((i64) nnew);
+            r.joins.push_back((i64) nj);
+            r.fulls.push_back((i64) (F.nbig + F.nsmall));
             if (nnew == 0) break;  // |full| unchanged
             if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
         }
+        settle(ctx, F);
+        nfull = F.nbig;
+        cur = F.cur;
     }
     pt.mark(PH_FINAL);
     DL_CUDA(cudaEventRecord(ev.b, ctx.stream));
@@ -391,6 +479,7 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     Graph g;
     u64 nfull = 0;
     int cur = 0;
+    FullSet F;
     if (n > 0) {
         rank_nodes(ctx, rows, n, g);
         ctx.reserve(ws.jbuf[0], n * 8);
@@ -411,7 +500,8 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         u64 nd = nvalid ? unique_words(ctx, b, nvalid, b) : 0;
         ctx.reserve(ws.full[0], std::max<u64>(nd, 1) * 8);
         if (nd) DL_CUDA(cudaMemcpyAsync(ws.full[0].p, b, nd * 8, cudaMemcpyDeviceToDevice, ctx.stream));
-        nfull = nd;
+        F.cur = 0;
+        F.nbig = nd;
         u64 *delta = b;
         u64 ndelta = nd;
         for (int it = 0;; ++it) {  // sg.cu:244-390
@@ -422,23 +512,18 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
             if (n1) {
                 u64 *j2 = join_and_sort(ctx, g, j1, n1, EmitKind::VZ, n2, nullptr, pt);  // (x, y)
                 pt.mark(PH_MERGE);
-                if (n2) {
-                    ctx.reserve(ws.full[1 - cur], (nfull + n2) * 8);
-                    DevBuf &dout = other(ws, j2);
-                    nnew = diff_merge_words(ctx, ws.full[cur].as<u64>(), nfull, j2, n2, ws.full[1 - cur].as<u64>(),
-                                            dout.as<u64>(), Codec::Raw);
-                    delta = dout.as<u64>();
-                    if (nnew) {
-                        cur = 1 - cur;
-                        nfull += nnew;
-                    }
-                }
+                delta = absorb(ctx, F, j2, n2, nnew);  // sg.cu:349-368
             }
             ndelta = nnew;
             r.deltas.push_back((i64) nnew);
+            r.joins.push_back((i64) (n1 + n2));
+            r.fulls.push_back((i64) (F.nbig + F.nsmall));
             if (nnew == 0) break;
             if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
         }
+        settle(ctx, F);
+        nfull = F.nbig;
+        cur = F.cur;
     }
     pt.mark(PH_FINAL);
     DL_CUDA(cudaEventRecord(ev.b, ctx.stream));
@@ -502,6 +587,8 @@ static void run_wcc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, bo
             std::swap(dcur, dnext);
             ndelta = nnew;
             r.deltas.push_back((i64) nnew);
+            r.joins.push_back((i64) total);
+            r.fulls.push_back((i64) nn);
             if (opt.wcc_stop == DL_WCC_STOP_FIXPOINT) {
                 if (nnew == 0) break;
             } else if ((i64) nnew == prev) {

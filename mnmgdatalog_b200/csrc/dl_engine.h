@@ -10,6 +10,8 @@ struct Run {
     dl_program program = DL_PROGRAM_TC;
     dl_run_info info{};
     std::vector<i64> deltas;  // |delta| after each iteration
+    std::vector<i64> joins;   // join output rows of each iteration
+    std::vector<i64> fulls;   // |full| after each iteration
     DevBuf words;             // TC/SG/single_join: sorted result words
     u64 n_words = 0;
     DevBuf ids;               // node id of each rank

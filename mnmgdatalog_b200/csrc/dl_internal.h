@@ -70,6 +70,7 @@ enum KernelId : int {
     K_DIFF_MERGE,      // fused unique/set-difference/merge: 8 B x (|full| + |J| + |full'| + |delta|)
     K_MERGE,           // plain merge: 16 B per word
     K_HASH_BUILD,      // C-ABI hash table insert / value extraction
+    K_SPARSE_DIFF,     // sparse set difference probes (+ run sampling)
     K_COUNT
 };
 const char *kernel_name(int kid);
@@ -87,7 +88,9 @@ struct Workspace {
     DevBuf ids;            // sorted distinct node ids (int32)
     DevBuf w0, w1;         // word buffers for the initial sorts
     DevBuf csr_off, csr_val;
-    DevBuf full[2];        // full relation, ping-pong
+    DevBuf full[2];        // full relation (large run), ping-pong
+    DevBuf small[2];       // full relation (small run), ping-pong
+    DevBuf sample;         // sample of the large run for sparse probes
     DevBuf jbuf[2];        // join output / sort ping-pong / delta
     DevBuf offsets;        // join count offsets
     DevBuf wcc_label, wcc_flag, wcc_next;
@@ -163,6 +166,9 @@ u64 unique_words(Context &ctx, const u64 *in, u64 n, u64 *out, int by_key_shift 
                  Codec codec = Codec::Raw);
 // Drops entity words whose key equals value. `out` may alias `in`.
 u64 remove_self_pairs_words(Context &ctx, const u64 *in, u64 n, u64 *out);
+// Drops all-ones words (the engine's "removed" marker). `out` may alias `in`.
+// `kind` is unused (reserved).
+u64 select_words(Context &ctx, const u64 *in, u64 n, u64 *out, int kind);
 
 // ---- merge path (dl_setops.cu) -------------------------------------------------
 // Stable merge (ties take `a` first), keeps duplicates: thrust::merge.
@@ -172,6 +178,13 @@ void merge_words(Context &ctx, const u64 *a, u64 na, const u64 *b, u64 nb, u64 *
 // null. Returns |delta|. full_out receives |full| + |delta| words.
 u64 diff_merge_words(Context &ctx, const u64 *full, u64 nfull, const u64 *j, u64 nj,
                      u64 *full_out, u64 *delta_out, Codec codec);
+// Sample of a sorted run for sparse_diff_words (every 4096th word).
+void run_sample(Context &ctx, const u64 *run, u64 n, DevBuf &sample, u64 &ns);
+// out = dedup(j) \ run for sorted j (duplicates allowed) and a sorted
+// duplicate-free run of compact words, by binary probes: O(|j| log) instead
+// of O(|run|). out may alias nothing in j/run; returns |out|.
+u64 sparse_diff_words(Context &ctx, const u64 *run, u64 nrun, const u64 *sample, u64 ns, const u64 *j, u64 nj,
+                      u64 *out);
 
 // ---- joins (dl_join.cu) --------------------------------------------------------
 struct Csr {            // relation grouped by dense key index

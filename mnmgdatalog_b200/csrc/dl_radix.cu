@@ -20,12 +20,12 @@ namespace {
 constexpr int RADIX = 256;
 constexpr int SORT_THREADS = 384;
 constexpr int SORT_WARPS = SORT_THREADS / 32;
-constexpr int SORT_KPT = 16;
-constexpr int SORT_TILE = SORT_THREADS * SORT_KPT;  // 6144 keys, 48 KiB
+constexpr int SORT_KPT_MAX = 16;
 constexpr int HIST_THREADS = 512;
 
+template <int KPT>
 struct SortSmem {
-    u64 keys[SORT_TILE];
+    u64 keys[SORT_THREADS * KPT];
     u32 warp_cnt[SORT_WARPS][RADIX];
     u32 match[SORT_WARPS][RADIX];  // peer masks of the atomicOr ranking
     u64 gbase[RADIX];
@@ -75,12 +75,14 @@ __global__ void __launch_bounds__(RADIX) radix_bucket_kernel(const u64 *__restri
 constexpr int RANK_BALLOT = 0;
 constexpr int RANK_ATOMIC = 1;
 
-template <bool ENC, bool DEC, int RANK>
-__global__ void __launch_bounds__(SORT_THREADS, 2)
+template <bool ENC, bool DEC, int RANK, int KPT, int MINB>
+__global__ void __launch_bounds__(SORT_THREADS, MINB)
 onesweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int shift,
                 const u64 *__restrict__ bucket, u64 *lb, u32 *tile_ctr, u32 epoch, u32 *err) {
+    constexpr int SORT_KPT = KPT;
+    constexpr int SORT_TILE = SORT_THREADS * KPT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SortSmem &s = *reinterpret_cast<SortSmem *>(smem_raw);
+    SortSmem<KPT> &s = *reinterpret_cast<SortSmem<KPT> *>(smem_raw);
     const int tid = threadIdx.x;
     const u32 lane = tid & 31;
     const int w = tid >> 5;
@@ -193,15 +195,36 @@ int rank_mode() {
     return mode;
 }
 
+// Keys per thread of a onesweep tile: DL_SORT_KPT=12|16 (default 16), read once.
+int sort_kpt() {
+    static int k = -1;
+    if (k < 0) {
+        const char *e = getenv("DL_SORT_KPT");
+        k = (e && std::string(e) == "12") ? 12 : 16;
+    }
+    return k;
+}
+
+template <bool ENC, bool DEC, int KPT, int MINB>
+void launch_onesweep_k(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, const u64 *bucket, u64 *lb, u32 *ctr) {
+    auto kern = rank_mode() == RANK_BALLOT ? onesweep_kernel<ENC, DEC, RANK_BALLOT, KPT, MINB>
+                                           : onesweep_kernel<ENC, DEC, RANK_ATOMIC, KPT, MINB>;
+    const int smem = (int) sizeof(SortSmem<KPT>);
+    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const u64 tile = (u64) SORT_THREADS * KPT;
+    const u64 tiles = (n + tile - 1) / tile;
+    DL_LAUNCH(ctx, K_SORT_PASS, 16.0 * n,
+              kern<<<(unsigned) tiles, SORT_THREADS, smem, ctx.stream>>>(in, out, n, shift, bucket, lb, ctr,
+                                                                          ctx.next_epoch(), &ctx.ctrl->err));
+}
+
+u64 sort_tile_keys() { return (u64) SORT_THREADS * sort_kpt(); }
+
 template <bool ENC, bool DEC>
 void launch_onesweep(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, const u64 *bucket, u64 *lb,
                      u32 *ctr) {
-    auto kern = rank_mode() == RANK_BALLOT ? onesweep_kernel<ENC, DEC, RANK_BALLOT>
-                                           : onesweep_kernel<ENC, DEC, RANK_ATOMIC>;
-    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(SortSmem)));
-    const u64 tiles = (n + SORT_TILE - 1) / SORT_TILE;
-    DL_LAUNCH(ctx, K_SORT_PASS, 16.0 * n, kern<<<(unsigned) tiles, SORT_THREADS, sizeof(SortSmem), ctx.stream>>>(in, out, n, shift, bucket, lb, ctr,
-                                                                          ctx.next_epoch(), &ctx.ctrl->err));
+    if (sort_kpt() == 12) launch_onesweep_k<ENC, DEC, 12, 3>(ctx, in, out, n, shift, bucket, lb, ctr);
+    else launch_onesweep_k<ENC, DEC, 16, 2>(ctx, in, out, n, shift, bucket, lb, ctr);
 }
 
 }  // namespace
@@ -248,7 +271,7 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
             if (!((m >> d) & 1u)) digits[nd++] = d;
     }
     if (nd == 0) return a;
-    const u64 tiles = (n + SORT_TILE - 1) / SORT_TILE;
+    const u64 tiles = (n + sort_tile_keys() - 1) / sort_tile_keys();
     u64 *lb = ctx.lookback_words(tiles * RADIX);
     const u64 *src = a;
     u64 *dst = b;

@@ -14,6 +14,11 @@ struct KeepRunHead {
     }
 };
 
+// Keep words other than the all-ones "removed" marker.
+struct KeepMarked {
+    __device__ bool operator()(u64 cur, u64, bool) const { return cur != ~0ull; }
+};
+
 // Keep Entity words whose key differs from their value.
 struct KeepNotSelfEntity {
     __device__ bool operator()(u64 cur, u64, bool) const { return (u32) cur != (u32) (cur >> 32); }
@@ -45,6 +50,10 @@ u64 unique_words(Context &ctx, const u64 *in, u64 n, u64 *out, int by_key_shift,
         mask = (codec == Codec::Entity) ? 0xFFFFFFFFull : (~0ull << by_key_shift);
     }
     return run_select(ctx, in, n, out, KeepRunHead{mask});
+}
+
+u64 select_words(Context &ctx, const u64 *in, u64 n, u64 *out, int) {
+    return run_select(ctx, in, n, out, KeepMarked{});
 }
 
 u64 remove_self_pairs_words(Context &ctx, const u64 *in, u64 n, u64 *out) {

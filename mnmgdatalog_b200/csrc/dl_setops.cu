@@ -259,6 +259,45 @@ merge_kernel(const u64 *__restrict__ a, u64 na, const u64 *__restrict__ b, u64 n
     for (u32 i = tid; i < la + lbn; i += MP_THREADS) out[d0 + i] = ENC ? entity_decode(s.buf[i]) : s.buf[i];
 }
 
+// Every SAMPLE_STRIDE-th word of a sorted run: a small L2-resident index
+// that narrows the binary search of a probe to one block of the run.
+constexpr u64 SAMPLE_STRIDE = 4096;
+
+__global__ void sample_kernel(const u64 *__restrict__ run, u64 n, u64 *__restrict__ sample, u64 ns) {
+    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (u64) gridDim.x * blockDim.x)
+        sample[i] = run[i * SAMPLE_STRIDE];
+}
+
+// Sparse set difference of sorted J (duplicates allowed) against a sorted
+// duplicate-free run: out[i] = J[i] if J[i] differs from J[i-1] and is not in
+// the run, else the all-ones word (never a compact tuple word). One thread per
+// J word: binary search of the sample, then of one 4096-word block.
+__global__ void sparse_mark_kernel(const u64 *__restrict__ j, u64 nj, const u64 *__restrict__ run, u64 nrun,
+                                   const u64 *__restrict__ sample, u64 ns, u64 *__restrict__ out) {
+    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < nj; i += (u64) gridDim.x * blockDim.x) {
+        const u64 b = j[i];
+        bool keep = (i == 0) || j[i - 1] != b;
+        if (keep && nrun) {
+            u64 lo = 0, hi = ns;  // last sample <= b
+            while (lo < hi) {
+                const u64 mid = (lo + hi) >> 1;
+                if (sample[mid] <= b) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo > 0) {
+                u64 l = (lo - 1) * SAMPLE_STRIDE, h = min(l + SAMPLE_STRIDE, nrun);
+                while (l < h) {
+                    const u64 mid = (l + h) >> 1;
+                    if (run[mid] < b) l = mid + 1;
+                    else h = mid;
+                }
+                keep = !(l < nrun && run[l] == b);
+            }
+        }
+        out[i] = keep ? b : ~0ull;
+    }
+}
+
 u64 *partition(Context &ctx, const u64 *a, u64 na, const u64 *b, u64 nb, Codec codec, u64 &tiles) {
     tiles = (na + nb + MP_TILE - 1) / MP_TILE;
     // Look-back words of the launch occupy [0, tiles + 1) of the context's
@@ -280,6 +319,26 @@ void launch_diff_merge(Context &ctx, const u64 *full, u64 nfull, const u64 *j, u
 }
 
 }  // namespace
+
+void run_sample(Context &ctx, const u64 *run, u64 n, DevBuf &sample, u64 &ns) {
+    ns = (n + SAMPLE_STRIDE - 1) / SAMPLE_STRIDE;
+    ctx.reserve(sample, std::max<u64>(ns, 1) * 8);
+    if (ns)
+        DL_LAUNCH(ctx, K_SPARSE_DIFF, 8.0 * ns,
+                  sample_kernel<<<(unsigned) std::min<u64>((ns + 255) / 256, 4096), 256, 0, ctx.stream>>>(
+                      run, n, sample.as<u64>(), ns));
+}
+
+u64 sparse_diff_words(Context &ctx, const u64 *run, u64 nrun, const u64 *sample, u64 ns, const u64 *j, u64 nj,
+                      u64 *out) {
+    if (nj == 0) return 0;
+    const unsigned grid = (unsigned) std::min<u64>((nj + 255) / 256, (u64) ctx.sm_count * 16);
+    // algorithmic bytes: J read + out written; the probes are counted as one
+    // 32-byte sector per J word
+    DL_LAUNCH(ctx, K_SPARSE_DIFF, 48.0 * nj,
+              sparse_mark_kernel<<<grid, 256, 0, ctx.stream>>>(j, nj, run, nrun, sample, ns, out));
+    return select_words(ctx, out, nj, out, 0);
+}
 
 void merge_words(Context &ctx, const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, Codec codec) {
     if (na + nb == 0) return;

@@ -50,6 +50,8 @@ class RunResult:
     largest_component: int = 0   # WCC
     join_rows_total: int = 0     # join output rows over all iterations (before dedup)
     join_rows_max: int = 0
+    join_rows: np.ndarray | None = None   # per iteration
+    full_rows: np.ndarray | None = None   # |full| after each iteration
     node_ids: np.ndarray | None = None
     labels: np.ndarray | None = None
 
@@ -168,6 +170,9 @@ class Engine:
             check(lib().dl_run_get_info(run, C.byref(info)))
             deltas = np.zeros(max(info.iterations, 0), dtype=np.int64)
             check(lib().dl_run_copy_deltas(run, deltas.ctypes.data, deltas.size))
+            jr = np.zeros(max(info.iterations, 1), dtype=np.int64)
+            fr = np.zeros(max(info.iterations, 1), dtype=np.int64)
+            check(lib().dl_run_copy_iteration_stats(run, jr.ctypes.data, fr.ctypes.data, jr.size))
             nout = info.output_rows
             rows = None
             if output == "host":
@@ -184,7 +189,8 @@ class Engine:
                 check(lib().dl_run_copy_output(run, C.c_void_p(rows.data_ptr()) if nout else None, nout, 1))
             res = RunResult(program, rows, info.iterations, deltas, info.output_tuples, info.nodes,
                             info.seconds_total, largest_component=info.largest_component,
-                            join_rows_total=info.join_rows_total, join_rows_max=info.join_rows_max)
+                            join_rows_total=info.join_rows_total, join_rows_max=info.join_rows_max,
+                            join_rows=jr[: len(deltas)], full_rows=fr[: len(deltas)])
             if phase_timing:
                 res.phases = {"initialization": info.seconds_init, "join": info.seconds_join,
                               "deduplication": info.seconds_dedup, "merge": info.seconds_merge,
