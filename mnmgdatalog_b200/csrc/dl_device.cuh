@@ -236,6 +236,47 @@ __device__ __forceinline__ u64 lookback_serial(const u64 *lb, u32 tile, u32 stri
     return excl;
 }
 
+// ---- TMA bulk copies (cp.async.bulk) with mbarrier completion ---------------
+__device__ __forceinline__ u32 smem_u32(const void *p) { return (u32) __cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(u64 *bar, u32 count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Arrive once and expect `bytes` of transaction on the barrier.
+__device__ __forceinline__ void mbar_expect_tx(u64 *bar, u32 bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_complete_tx(u64 *bar, u32 bytes) {
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// 1D bulk copy global -> shared; dst, src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void tma_load_1d(void *dst, const void *src, u32 bytes, u64 *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(u64 *bar, u32 phase) {
+    u32 ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for a barrier phase; returns false (and flags `err`) on timeout.
+__device__ __forceinline__ bool mbar_wait(u64 *bar, u32 phase, u32 *err) {
+    u32 spins = 0;
+    while (!mbar_try_wait(bar, phase)) {
+        if (++spins > kSpinLimit) {
+            atomicOr(err, DL_DEVERR_LOOKBACK);
+            return false;
+        }
+    }
+    return true;
+}
+
 __device__ __forceinline__ u32 fmix32(u32 k) {
     // MurmurHash3 finalizer; same mixing as the reference's get_position
     // (common/utils.cu:149-156).

@@ -264,9 +264,10 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
     ctx.reserve(jout, std::max<u64>(total, 1) * 8);
     if (total == 0) return jout.as<u64>();
     const int key_bits = 2 * g.bits;
-    const int ndig = (key_bits + 7) / 8;
-    u64 *hist = radix_hist_buffer(ctx);
-    radix_hist_clear(ctx);
+    const bool fuse_hist = radix_wants_histogram();
+    const int ndig = fuse_hist ? (key_bits + 7) / 8 : 0;
+    u64 *hist = fuse_hist ? radix_hist_buffer(ctx) : nullptr;
+    if (fuse_hist) radix_hist_clear(ctx);
     join_emit(ctx, g.csr, probe, n_probe, g.bits, ws.offsets.as<u64>(), total, kind, jout.as<u64>(), hist, ndig,
               self_pairs);
     pt.mark(PH_DEDUP);

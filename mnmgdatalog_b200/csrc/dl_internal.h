@@ -106,6 +106,7 @@ struct Context {
     DevBuf lookback;                // look-back words (zeroed at allocation)
     DevBuf sort_hist;               // radix histograms / bucket bases
     DevBuf lbs_splits;              // join emit partition points
+    DevBuf radix_part;              // per-(digit, CTA) counts and offsets of a radix pass
     u64 *host_scalars = nullptr;    // pinned mirror for small D2H reads
     Workspace ws;
     u64 run_join_total = 0, run_join_max = 0;  // join statistics of the current run
@@ -157,6 +158,9 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
 // into ctx.sort_hist; lets radix_sort skip its own histogram pass.
 u64 *radix_hist_buffer(Context &ctx);
 void radix_hist_clear(Context &ctx);
+// True when radix_sort benefits from a producer-accumulated histogram
+// (the onesweep variant); the three-kernel variant counts per chunk itself.
+bool radix_wants_histogram();
 
 // ---- compaction / scan (dl_scan.cu) ------------------------------------------
 // out[i] = in[i] for the first of each run of equal words; returns count.

@@ -13,6 +13,7 @@
 // HBM traffic per pass: 8 B read + 8 B written per key (+ 8 B read once for
 // the histogram unless a producer kernel accumulated it while writing).
 #include "dl_internal.h"
+#include "dl_scan.cuh"
 
 namespace dl {
 namespace {
@@ -227,6 +228,228 @@ void launch_onesweep(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, co
     else launch_onesweep_k<ENC, DEC, 16, 2>(ctx, in, out, n, shift, bucket, lb, ctr);
 }
 
+// ---- three-kernel LSD pass: upsweep / spine / downsweep ---------------------
+// A pass without inter-CTA waits: CTA c owns a contiguous chunk of keys. The
+// upsweep counts the chunk's digits, a scan over the digit-major [256][G]
+// matrix gives every (digit, CTA) its first output position, and the
+// downsweep streams the chunk tile by tile (TMA bulk loads, double-buffered
+// behind an mbarrier) keeping a running offset per digit. Traffic per pass:
+// 8 B (upsweep) + 16 B (downsweep) per key.
+constexpr int DS_THREADS = 256;
+constexpr int DS_WARPS = DS_THREADS / 32;
+constexpr int DS_KPT = 16;
+constexpr int DS_TILE = DS_THREADS * DS_KPT;  // 4096 keys, 32 KiB
+constexpr int US_THREADS = 512;
+
+struct DsSmem {
+    u64 buf[2][DS_TILE];  // TMA landing buffers; the current one also stages the scatter
+    u32 warp_cnt[DS_WARPS][RADIX];
+    u32 match[DS_WARPS][RADIX];
+    u64 run_off[RADIX];
+    u64 gbase[RADIX];
+    u32 tile_start[RADIX];
+    u32 scratch[DS_WARPS + 1];
+    u64 bar[2];
+};
+
+template <bool ENC>
+__global__ void __launch_bounds__(US_THREADS)
+radix_upsweep_kernel(const u64 *__restrict__ in, u64 n, int shift, u64 chunk, u32 G, u64 *__restrict__ hist) {
+    __shared__ u32 h[US_THREADS / 32][RADIX];
+    const int tid = threadIdx.x, w = tid >> 5;
+    for (int i = tid; i < (US_THREADS / 32) * RADIX; i += US_THREADS) (&h[0][0])[i] = 0;
+    __syncthreads();
+    const u64 b = (u64) blockIdx.x * chunk;
+    const u64 e = min(b + chunk, n);
+    u64 i = b + tid;
+    for (; i + 3 * US_THREADS < e; i += 4 * US_THREADS) {
+        u64 k0 = __ldcs(in + i), k1 = __ldcs(in + i + US_THREADS), k2 = __ldcs(in + i + 2 * US_THREADS),
+            k3 = __ldcs(in + i + 3 * US_THREADS);
+        if (ENC) {
+            k0 = entity_encode(k0);
+            k1 = entity_encode(k1);
+            k2 = entity_encode(k2);
+            k3 = entity_encode(k3);
+        }
+        atomicAdd(&h[w][(k0 >> shift) & 255u], 1u);
+        atomicAdd(&h[w][(k1 >> shift) & 255u], 1u);
+        atomicAdd(&h[w][(k2 >> shift) & 255u], 1u);
+        atomicAdd(&h[w][(k3 >> shift) & 255u], 1u);
+    }
+    for (; i < e; i += US_THREADS) {
+        u64 k = __ldcs(in + i);
+        if (ENC) k = entity_encode(k);
+        atomicAdd(&h[w][(k >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (tid < RADIX) {
+        u32 sum = 0;
+#pragma unroll
+        for (int ww = 0; ww < US_THREADS / 32; ++ww) sum += h[ww][tid];
+        hist[(u64) tid * G + blockIdx.x] = sum;
+    }
+}
+
+struct WordValue {
+    const u64 *v;
+    __device__ __forceinline__ u64 operator()(u64 i) const { return v[i]; }
+};
+
+template <bool ENC, bool DEC>
+__global__ void __launch_bounds__(DS_THREADS, 2)
+radix_downsweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int shift, u64 chunk, u32 G,
+                       const u64 *__restrict__ offsets, int use_tma, u32 *err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    DsSmem &s = *reinterpret_cast<DsSmem *>(smem_raw);
+    const int tid = threadIdx.x;
+    const u32 lane = tid & 31;
+    const int w = tid >> 5;
+    const u64 cb = (u64) blockIdx.x * chunk;
+    if (cb >= n) return;
+    const u64 ce = min(cb + chunk, n);
+    const u32 ntiles = (u32) ((ce - cb + DS_TILE - 1) / DS_TILE);
+    if (tid < RADIX) s.run_off[tid] = offsets[(u64) tid * G + blockIdx.x];
+    for (int i = tid; i < DS_WARPS * RADIX; i += DS_THREADS) {
+        (&s.warp_cnt[0][0])[i] = 0;
+        (&s.match[0][0])[i] = 0;
+    }
+    auto issue = [&](u32 t, int slot) {  // thread 0 only
+        const u64 tb = cb + (u64) t * DS_TILE;
+        const u32 cnt = (u32) min((u64) DS_TILE, ce - tb);
+        const u32 bytes = (cnt * 8u) & ~15u;
+        mbar_expect_tx(&s.bar[slot], bytes ? bytes : 16u);
+        if (bytes) tma_load_1d(s.buf[slot], in + tb, bytes, &s.bar[slot]);
+        else mbar_complete_tx(&s.bar[slot], 16u);
+    };
+    if (use_tma && tid == 0) {
+        mbar_init(&s.bar[0], 1);
+        mbar_init(&s.bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (use_tma && tid == 0) {
+        issue(0, 0);
+        if (ntiles > 1) issue(1, 1);
+    }
+    u32 phase0 = 0, phase1 = 0;
+    const u32 lt = lanemask_lt();
+    for (u32 t = 0; t < ntiles; ++t) {
+        const int slot = t & 1;
+        u64 *buf = s.buf[slot];
+        const u64 tb = cb + (u64) t * DS_TILE;
+        const u32 cnt = (u32) min((u64) DS_TILE, ce - tb);
+        u32 tma_words = 0;
+        if (use_tma) {
+            tma_words = ((cnt * 8u) & ~15u) / 8u;
+            if (slot == 0) {
+                mbar_wait(&s.bar[0], phase0, err);
+                phase0 ^= 1;
+            } else {
+                mbar_wait(&s.bar[1], phase1, err);
+                phase1 ^= 1;
+            }
+        }
+        u64 k[DS_KPT];
+        const u32 wb = (u32) w * 32 * DS_KPT + lane;
+#pragma unroll
+        for (int i = 0; i < DS_KPT; ++i) {
+            const u32 li = wb + i * 32;
+            if (li < cnt) {
+                const u64 x = li < tma_words ? buf[li] : __ldcs(in + tb + li);
+                k[i] = ENC ? entity_encode(x) : x;
+            } else {
+                k[i] = ~0ull;
+            }
+        }
+        u32 rank[DS_KPT];
+#pragma unroll
+        for (int i = 0; i < DS_KPT; ++i) {
+            const u32 d = (u32) (k[i] >> shift) & 255u;
+            atomicOr(&s.match[w][d], 1u << lane);
+            __syncwarp();
+            const u32 peers = *reinterpret_cast<volatile u32 *>(&s.match[w][d]);
+            __syncwarp();
+            const u32 leader = __ffs(peers) - 1;
+            u32 prev = 0;
+            if (lane == leader) {
+                prev = s.warp_cnt[w][d];
+                s.warp_cnt[w][d] = prev + __popc(peers);
+                s.match[w][d] = 0;
+            }
+            __syncwarp();
+            prev = __shfl_sync(0xffffffffu, prev, leader);
+            rank[i] = prev + __popc(peers & lt);
+        }
+        __syncthreads();  // ranks done; the landing buffer is no longer read
+        u32 cnt_all = 0, cnt_valid = 0;
+        if (tid < RADIX) {
+            u32 sum = 0;
+#pragma unroll
+            for (int ww = 0; ww < DS_WARPS; ++ww) {
+                const u32 c = s.warp_cnt[ww][tid];
+                s.warp_cnt[ww][tid] = sum;
+                sum += c;
+            }
+            cnt_all = sum;
+            cnt_valid = (tid == RADIX - 1) ? sum - (DS_TILE - cnt) : sum;
+        }
+        u32 total;
+        const u32 start = block_exclusive_sum<DS_WARPS>(tid < RADIX ? cnt_all : 0u, s.scratch, &total);
+        if (tid < RADIX) {
+            s.tile_start[tid] = start;
+            s.gbase[tid] = s.run_off[tid] - start;
+            s.run_off[tid] += cnt_valid;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < DS_KPT; ++i) {
+            const u32 d = (u32) (k[i] >> shift) & 255u;
+            buf[s.tile_start[d] + s.warp_cnt[w][d] + rank[i]] = k[i];
+        }
+        __syncthreads();
+        if (tid < RADIX)
+#pragma unroll
+            for (int ww = 0; ww < DS_WARPS; ++ww) s.warp_cnt[ww][tid] = 0;
+        for (u32 j = tid; j < cnt; j += DS_THREADS) {
+            const u64 x = buf[j];
+            const u32 d = (u32) (x >> shift) & 255u;
+            out[s.gbase[d] + j] = DEC ? entity_decode(x) : x;
+        }
+        __syncthreads();  // buffer and counters free for the next tiles
+        if (use_tma && tid == 0 && t + 2 < ntiles) issue(t + 2, slot);
+    }
+}
+
+// Sort algorithm: DL_SORT_ALGO=onesweep|lsd3 (default lsd3), read once.
+bool use_lsd3() {
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("DL_SORT_ALGO");
+        v = (e && std::string(e) == "onesweep") ? 0 : 1;
+    }
+    return v == 1;
+}
+
+template <bool ENC, bool DEC>
+void lsd3_pass(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, u32 G, u64 chunk, u64 *hist, u64 *offs) {
+    DL_LAUNCH(ctx, K_SORT_HIST, 8.0 * n,
+              radix_upsweep_kernel<ENC><<<G, US_THREADS, 0, ctx.stream>>>(in, n, shift, chunk, G, hist));
+    const u64 m = (u64) RADIX * G;
+    const u64 tiles = (m + SCAN_TILE - 1) / SCAN_TILE;
+    u64 *lb = ctx.lookback_words(tiles);
+    u32 *ctr = ctx.tile_counter(56);
+    DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(u32), ctx.stream));
+    DL_LAUNCH(ctx, K_SORT_BUCKET, 16.0 * m,
+              scan_kernel<WordValue><<<(unsigned) tiles, SCAN_THREADS, 0, ctx.stream>>>(
+                  WordValue{hist}, m, offs, lb, ctr, ctx.next_epoch(), &ctx.ctrl->err, &ctx.ctrl->scalar[12]));
+    auto kern = radix_downsweep_kernel<ENC, DEC>;
+    const int smem = (int) sizeof(DsSmem);
+    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int use_tma = ((reinterpret_cast<uintptr_t>(in) & 15u) == 0) ? 1 : 0;
+    DL_LAUNCH(ctx, K_SORT_PASS, 16.0 * n,
+              kern<<<G, DS_THREADS, smem, ctx.stream>>>(in, out, n, shift, chunk, G, offs, use_tma, &ctx.ctrl->err));
+}
+
 }  // namespace
 
 // Histogram bins [8][256] followed by bucket bases [8][256].
@@ -250,31 +473,59 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
     int nd = 0;
     DL_CUDA(cudaMemsetAsync(ctr, 0, 17 * sizeof(u32), ctx.stream));
     const int ndig = (known_bits > 0 && !ent) ? (known_bits + 7) / 8 : 8;
-    const unsigned hgrid = (unsigned) std::min<u64>((n + HIST_THREADS * 8 - 1) / (HIST_THREADS * 8),
-                                                    (u64) ctx.sm_count * 4);
-    if (!hist_accumulated) {
-        radix_hist_clear(ctx);
-        if (ent)
-            DL_LAUNCH(ctx, K_SORT_HIST, 8.0 * n, radix_hist_kernel<true><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist));
-        else
-            DL_LAUNCH(ctx, K_SORT_HIST, 8.0 * n, radix_hist_kernel<false><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist));
-    }
-    DL_LAUNCH(ctx, K_SORT_BUCKET, 0, radix_bucket_kernel<<<ndig, RADIX, 0, ctx.stream>>>(hist, bucket, n, mask));
+    const bool lsd3 = use_lsd3();
     if (known_bits > 0 && !ent) {
         for (int d = 0; d < ndig; ++d) digits[nd++] = d;
-    } else {
-        u32 m = 0;
-        DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, mask, sizeof(u32), cudaMemcpyDeviceToHost, ctx.stream));
-        ctx.sync();
-        m = *reinterpret_cast<u32 *>(ctx.host_scalars);
-        for (int d = 0; d < 8; ++d)
-            if (!((m >> d) & 1u)) digits[nd++] = d;
+    }
+    if (!(known_bits > 0 && !ent) || !lsd3) {
+        const unsigned hgrid = (unsigned) std::min<u64>((n + HIST_THREADS * 8 - 1) / (HIST_THREADS * 8),
+                                                        (u64) ctx.sm_count * 4);
+        if (!hist_accumulated) {
+            radix_hist_clear(ctx);
+            if (ent)
+                DL_LAUNCH(ctx, K_SORT_HIST, 8.0 * n,
+                          radix_hist_kernel<true><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist));
+            else
+                DL_LAUNCH(ctx, K_SORT_HIST, 8.0 * n,
+                          radix_hist_kernel<false><<<hgrid, HIST_THREADS, 0, ctx.stream>>>(a, n, ndig, hist));
+        }
+        DL_LAUNCH(ctx, K_SORT_BUCKET, 0,
+                  radix_bucket_kernel<<<ndig, RADIX, 0, ctx.stream>>>(hist, bucket, n, mask));
+        if (!(known_bits > 0 && !ent)) {
+            DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, mask, sizeof(u32), cudaMemcpyDeviceToHost, ctx.stream));
+            ctx.sync();
+            const u32 m = *reinterpret_cast<u32 *>(ctx.host_scalars);
+            for (int d = 0; d < 8; ++d)
+                if (!((m >> d) & 1u)) digits[nd++] = d;
+        }
     }
     if (nd == 0) return a;
-    const u64 tiles = (n + sort_tile_keys() - 1) / sort_tile_keys();
-    u64 *lb = ctx.lookback_words(tiles * RADIX);
     const u64 *src = a;
     u64 *dst = b;
+    if (lsd3) {
+        u64 G = std::min<u64>((u64) ctx.sm_count * 2, (n + DS_TILE - 1) / DS_TILE);
+        if (G == 0) G = 1;
+        u64 chunk = (n + G - 1) / G;
+        chunk = (chunk + DS_TILE - 1) / DS_TILE * DS_TILE;
+        G = (n + chunk - 1) / chunk;
+        ctx.reserve(ctx.radix_part, 2 * RADIX * G * sizeof(u64));
+        u64 *ph = ctx.radix_part.as<u64>();
+        u64 *po = ph + RADIX * G;
+        for (int p = 0; p < nd; ++p) {
+            const bool enc = ent && p == 0, dec = ent && p == nd - 1;
+            const int sh = 8 * digits[p];
+            if (enc && dec) lsd3_pass<true, true>(ctx, src, dst, n, sh, (u32) G, chunk, ph, po);
+            else if (enc) lsd3_pass<true, false>(ctx, src, dst, n, sh, (u32) G, chunk, ph, po);
+            else if (dec) lsd3_pass<false, true>(ctx, src, dst, n, sh, (u32) G, chunk, ph, po);
+            else lsd3_pass<false, false>(ctx, src, dst, n, sh, (u32) G, chunk, ph, po);
+            u64 *t = const_cast<u64 *>(src);
+            src = dst;
+            dst = t;
+        }
+        return const_cast<u64 *>(src);
+    }
+    const u64 tiles = (n + sort_tile_keys() - 1) / sort_tile_keys();
+    u64 *lb = ctx.lookback_words(tiles * RADIX);
     for (int p = 0; p < nd; ++p) {
         const bool enc = ent && p == 0, dec = ent && p == nd - 1;
         const u64 *bk = bucket + digits[p] * RADIX;
@@ -289,5 +540,7 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
     }
     return const_cast<u64 *>(src);
 }
+
+bool radix_wants_histogram() { return !use_lsd3(); }
 
 }  // namespace dl
