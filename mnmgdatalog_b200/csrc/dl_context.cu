@@ -111,7 +111,7 @@ void Context::check_device_error() {
 }
 
 const char *kernel_name(int kid) {
-    static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_bucket_scan", "sort_onesweep_pass",
+    static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_spine_scan", "sort_scatter_pass",
                                          "select_compact", "join_count_scan", "join_partition", "join_emit",
                                          "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build",
                                          "sparse_diff"};

@@ -58,9 +58,9 @@ struct DevBuf {
 // events on the context stream, algorithmic HBM bytes).
 enum KernelId : int {
     K_PREP = 0,        // init / finalize transforms (pack, rank, CSR, unpack)
-    K_SORT_HIST,       // radix histogram pass
-    K_SORT_BUCKET,     // radix bucket scan
-    K_SORT_PASS,       // onesweep radix pass: 16 B per key
+    K_SORT_HIST,       // radix histogram (upsweep): 8 B per key
+    K_SORT_BUCKET,     // radix spine scan of the (digit, CTA) counts
+    K_SORT_PASS,       // radix scatter pass (downsweep or onesweep): 16 B per key
     K_SELECT,          // unique / remove_if compaction: 8 B read + 8 B per kept word
     K_JOIN_COUNT,      // join count + scan: 8 B probe read + 8 B offset write per probe row
     K_JOIN_PARTITION,  // merge-path partition of the emit
