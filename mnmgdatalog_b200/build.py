@@ -21,6 +21,9 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libmnmgdl.so")
+BIN = os.path.join(PKG, "bin")
+CLI_SRC = os.path.join(PKG, "cli", "dl_cli.cpp")
+CLI_PROGRAMS = {"tc": 0, "sg": 1, "wcc": 2, "single_join": 3}
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -71,9 +74,28 @@ def build(force: bool = False, extra: list[str] | None = None, verbose: bool = F
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_cli(force)
     if verbose:
         print(LIB)
     return LIB
+
+
+def build_cli(force: bool = False) -> list[str]:
+    """The reference-compatible command-line programs (mnmgdatalog_b200/bin/)."""
+    os.makedirs(BIN, exist_ok=True)
+    cxx = shutil.which("g++") or "g++"
+    outs = []
+    for name, prog in CLI_PROGRAMS.items():
+        exe = os.path.join(BIN, name)
+        newest = max(os.path.getmtime(CLI_SRC), os.path.getmtime(LIB), os.path.getmtime(os.path.join(INCLUDE, "mnmgdl.h")))
+        if force or not os.path.exists(exe) or os.path.getmtime(exe) < newest:
+            cmd = [cxx, "-O2", "-std=c++17", f"-DDL_CLI_PROGRAM={prog}", "-I", INCLUDE, CLI_SRC, "-o", exe,
+                   "-L", PKG, "-lmnmgdl", "-Wl,-rpath,$ORIGIN/.."]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"CLI build failed:\n{r.stdout}\n{r.stderr}")
+        outs.append(exe)
+    return outs
 
 
 def main(argv: list[str] | None = None) -> int:

@@ -32,6 +32,7 @@ EXPORTS = (
     "dl_run_get_info", "dl_run_copy_output", "dl_run_copy_deltas", "dl_run_copy_labels", "dl_run_destroy",
     "dl_run_copy_iteration_stats",
     "dl_generate_rows", "dl_profile_enable", "dl_profile_read",
+    "dl_compat_get_hash_table", "dl_compat_get_join", "dl_compat_get_join_nl",
 )
 
 

@@ -11,7 +11,7 @@ from conftest import ROOT
 
 def _declared_symbols():
     names = set()
-    for h in ("mnmgdl.h",):
+    for h in ("mnmgdl.h", "mnmgdl_compat.h"):
         txt = open(os.path.join(ROOT, "include", h)).read()
         names |= set(re.findall(r"DL_API[^;(]*?\b(dl_[a-z0-9_]+)\s*\(", txt))
     return names
