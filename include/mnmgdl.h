@@ -136,6 +136,21 @@ DL_API dl_status dl_unique_by_key_min(dl_context *ctx, dl_entity *rel, int64_t n
 /* Drop rows with key == value, order kept. */
 DL_API dl_status dl_remove_self_pairs(dl_context *ctx, dl_entity *rel, int64_t n, int64_t *n_out);
 
+/* dl_sort_unique without any memory allocation. No counterpart in the
+ * reference. For callers that cannot call cudaMalloc at sort time -- device
+ * memory already owned by another allocator's pool, a fixed device footprint
+ * after start-up, or no room for the device-wide synchronisation an
+ * allocation can cause. Scratch comes from a fixed device array built into
+ * the library (about 10 MiB on every GPU that loads it, held until the
+ * process exits), so at most dl_sort_unique_noalloc_max_rows() rows
+ * (1,048,576) are accepted; more is DL_ERR_INVALID_ARGUMENT. `stream` is a
+ * cudaStream_t (NULL = default stream); the call returns after its GPU work
+ * is done. The first call on a device looks the array up (set-up) and should
+ * come before any stream capture. All calls share the array: calls whose GPU
+ * work overlapped would race, so concurrent host calls are serialised. */
+DL_API dl_status dl_sort_unique_noalloc(dl_entity *rel, int64_t n, int64_t *n_out, void *stream);
+DL_API int64_t dl_sort_unique_noalloc_max_rows(void);
+
 /* ---- hash table and joins ---- */
 
 /* Index a relation by key. load_factor <= 0 selects the default (0.5). The

@@ -33,6 +33,7 @@ EXPORTS = (
     "dl_run_copy_iteration_stats",
     "dl_generate_rows", "dl_profile_enable", "dl_profile_read",
     "dl_compat_get_hash_table", "dl_compat_get_join", "dl_compat_get_join_nl",
+    "dl_sort_unique_noalloc", "dl_sort_unique_noalloc_max_rows",
 )
 
 
@@ -107,6 +108,8 @@ def lib():
         "dl_run_destroy": ([vp], C.c_int),
         "dl_generate_rows": ([i64, i32, C.c_uint32, vp], C.c_int),
         "dl_profile_enable": ([vp, i32], C.c_int),
+        "dl_sort_unique_noalloc": ([vp, i64, pi64, vp], C.c_int),
+        "dl_sort_unique_noalloc_max_rows": ([], C.c_int64),
         "dl_profile_read": ([vp, C.POINTER(dl_kernel_stat), i32, C.POINTER(C.c_int32)], C.c_int),
     }
     for name, (args, res) in sig.items():

@@ -84,6 +84,11 @@ struct GlibcRand {
 
 }  // namespace
 
+namespace dl {
+// Error text for dl_last_error() from entry points defined in other files.
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace dl
+
 extern "C" {
 
 DL_API const char *dl_status_string(dl_status s) {

@@ -16,6 +16,9 @@
 
 namespace dl {
 
+// Sets the calling thread's dl_last_error() text.
+void set_last_error(const std::string &msg);
+
 // Error raised inside the engine; the C-ABI layer converts it to a dl_status.
 struct Error : std::runtime_error {
     dl_status status;
