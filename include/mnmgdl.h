@@ -201,6 +201,51 @@ DL_API dl_status dl_run_copy_iteration_stats(const dl_run *run, int64_t *join_ro
 DL_API dl_status dl_run_copy_labels(const dl_run *run, int32_t *node_ids, int32_t *labels, int64_t capacity);
 DL_API dl_status dl_run_destroy(dl_run *run);
 
+/* ---- sessions: many fixpoint instances at once (batched and served forms) ----
+ *
+ * No counterpart in the reference, whose drivers run one program on one
+ * edge file per process (tc.cu:42-423, sg.cu:40-477, wcc.cu:58-585). A
+ * session runs every admitted instance of one program (TC, SG or WCC) as one
+ * union fixpoint: each iteration's joins, sorts, set difference and merge
+ * process all active instances in the same launches. Instances can be
+ * admitted between any two steps (continuous batching) and leave the union
+ * at their own fixpoint. Each instance's outputs, iteration count and delta
+ * sizes are those of dl_run_program on the same edges and options.
+ * A session owns device memory on its context's device and stream; calls on
+ * one session must not run concurrently. */
+typedef struct dl_session dl_session;
+
+/* max_nodes bounds the node count of the instances alive at once (TC/SG
+ * words then carry 2 * ceil(log2(max_nodes)) bits; 0 = 2^30). */
+DL_API dl_status dl_session_create(dl_context *ctx, int32_t program, const dl_options *opts, int64_t max_nodes,
+                                   dl_session **out);
+/* Adds an instance on `rows` int32 edge pairs; *instance receives its id
+ * (ids count up from 0). Its first iteration runs in the next step. An
+ * instance with no edges finishes at once. */
+DL_API dl_status dl_session_admit(dl_session *s, const int32_t *edges, int64_t rows, int32_t edges_on_device,
+                                  int64_t *instance);
+/* One iteration of every active instance; *active = instances still running. */
+DL_API dl_status dl_session_step(dl_session *s, int64_t *active);
+/* Ids of the instances finished since the last poll, in finishing order;
+ * at most `capacity` are returned and the rest stay queued. */
+DL_API dl_status dl_session_poll(dl_session *s, int64_t *ids, int64_t capacity, int64_t *count);
+DL_API dl_status dl_session_get_info(const dl_session *s, int64_t instance, dl_run_info *info);
+/* Same layouts as dl_run_copy_output / dl_run_copy_deltas / dl_run_copy_labels. */
+DL_API dl_status dl_session_copy_output(dl_session *s, int64_t instance, int32_t *dst, int64_t capacity_rows,
+                                        int32_t dst_on_device);
+DL_API dl_status dl_session_copy_deltas(const dl_session *s, int64_t instance, int64_t *dst, int64_t capacity);
+DL_API dl_status dl_session_copy_labels(dl_session *s, int64_t instance, int32_t *node_ids, int32_t *labels,
+                                        int64_t capacity);
+/* Frees a finished instance's result memory (its info stays readable). */
+DL_API dl_status dl_session_release(dl_session *s, int64_t instance);
+/* Device bytes held by the session and the number of active instances. */
+DL_API dl_status dl_session_memory(const dl_session *s, int64_t *device_bytes, int64_t *active);
+DL_API dl_status dl_session_destroy(dl_session *s);
+/* Batched form: admits `count` edge sets (edges[i] holds rows[i] pairs) and
+ * steps until every instance has finished; results are read from *out. */
+DL_API dl_status dl_run_batch(dl_context *ctx, int32_t program, const int32_t *const *edges, const int64_t *rows,
+                              int64_t count, int32_t edges_on_device, const dl_options *opts, dl_session **out);
+
 /* ---- live kernel profile (CUDA events on the context stream) ---- */
 
 typedef struct dl_kernel_stat {

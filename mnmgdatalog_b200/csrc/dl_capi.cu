@@ -5,6 +5,7 @@
 #include "dl_engine.h"
 #include "dl_internal.h"
 #include "dl_join.cuh"
+#include "dl_session.h"
 
 struct dl_context {
     dl::Context c;
@@ -15,6 +16,10 @@ struct dl_hash_table {
 };
 struct dl_run {
     dl::Run *r = nullptr;
+};
+struct dl_session {
+    dl::SessionImpl *s = nullptr;
+    dl_context *ctx = nullptr;
 };
 
 namespace {
@@ -436,6 +441,143 @@ DL_API dl_status dl_run_destroy(dl_run *run) {
         dl::run_destroy(run->r);
     }
     delete run;
+    return DL_OK;
+}
+
+// ---- sessions (dl_session.cu) ----
+
+DL_API dl_status dl_session_create(dl_context *ctx, int32_t program, const dl_options *opts, int64_t max_nodes,
+                                   dl_session **out) {
+    DL_REQUIRE(ctx && out && max_nodes >= 0, "invalid argument");
+    DL_REQUIRE(program == DL_PROGRAM_TC || program == DL_PROGRAM_SG || program == DL_PROGRAM_WCC,
+               "sessions run TC, SG or WCC");
+    *out = nullptr;
+    dl_options o{};
+    if (opts) o = *opts;
+    DL_REQUIRE(o.wcc_stop == DL_WCC_STOP_REFERENCE || o.wcc_stop == DL_WCC_STOP_FIXPOINT, "unknown wcc_stop");
+    auto s = std::make_unique<dl_session>();
+    s->ctx = ctx;
+    dl_status st = guarded([&] {
+        set_device(ctx);
+        s->s = dl::session_create(ctx->c, program, o, (u64) max_nodes);
+    });
+    if (st == DL_OK) *out = s.release();
+    return st;
+}
+
+DL_API dl_status dl_session_admit(dl_session *s, const int32_t *edges, int64_t rows, int32_t edges_on_device,
+                                  int64_t *instance) {
+    DL_REQUIRE(s && s->s && instance && rows >= 0 && (edges || rows == 0), "invalid argument");
+    DL_REQUIRE(rows <= (int64_t) 0x7FFFFFFF, "more than 2^31-1 input rows");
+    return guarded([&] {
+        set_device(s->ctx);
+        *instance = dl::session_admit(*s->s, edges, (u64) rows, edges_on_device != 0);
+        dl::session_fold_profile(*s->s, s->ctx->c);
+    });
+}
+
+DL_API dl_status dl_session_step(dl_session *s, int64_t *active) {
+    DL_REQUIRE(s && s->s, "invalid argument");
+    return guarded([&] {
+        set_device(s->ctx);
+        const u64 a = dl::session_step(*s->s);
+        dl::session_fold_profile(*s->s, s->ctx->c);
+        if (active) *active = (int64_t) a;
+    });
+}
+
+DL_API dl_status dl_session_poll(dl_session *s, int64_t *ids, int64_t capacity, int64_t *count) {
+    DL_REQUIRE(s && s->s && count && capacity >= 0 && (ids || capacity == 0), "invalid argument");
+    return guarded([&] { *count = (int64_t) dl::session_poll(*s->s, ids, (u64) capacity); });
+}
+
+DL_API dl_status dl_session_get_info(const dl_session *s, int64_t instance, dl_run_info *info) {
+    DL_REQUIRE(s && s->s && info, "invalid argument");
+    return guarded([&] { dl::session_info(*s->s, instance, *info); });
+}
+
+DL_API dl_status dl_session_copy_output(dl_session *s, int64_t instance, int32_t *dst, int64_t capacity_rows,
+                                        int32_t dst_on_device) {
+    DL_REQUIRE(s && s->s && capacity_rows >= 0, "invalid argument");
+    return guarded([&] {
+        set_device(s->ctx);
+        if (!dst && dl::session_instance(*s->s, instance).n_result)
+            throw dl::Error(DL_ERR_INVALID_ARGUMENT, "dst is NULL");
+        dl::session_copy_output(*s->s, instance, dst, (u64) capacity_rows, dst_on_device != 0);
+    });
+}
+
+DL_API dl_status dl_session_copy_deltas(const dl_session *s, int64_t instance, int64_t *dst, int64_t capacity) {
+    DL_REQUIRE(s && s->s && capacity >= 0, "invalid argument");
+    return guarded([&] {
+        const auto &d = dl::session_instance(*s->s, instance).deltas;
+        if ((int64_t) d.size() > capacity)
+            throw dl::Error(DL_ERR_INVALID_ARGUMENT, "delta capacity smaller than the iteration count");
+        if (!d.empty()) std::memcpy(dst, d.data(), d.size() * sizeof(int64_t));
+    });
+}
+
+DL_API dl_status dl_session_copy_labels(dl_session *s, int64_t instance, int32_t *node_ids, int32_t *labels,
+                                        int64_t capacity) {
+    DL_REQUIRE(s && s->s && capacity >= 0, "invalid argument");
+    return guarded([&] {
+        set_device(s->ctx);
+        if ((!node_ids || !labels) && dl::session_instance(*s->s, instance).n_ids)
+            throw dl::Error(DL_ERR_INVALID_ARGUMENT, "node_ids/labels is NULL");
+        dl::session_copy_labels(*s->s, instance, node_ids, labels, (u64) capacity);
+    });
+}
+
+DL_API dl_status dl_session_release(dl_session *s, int64_t instance) {
+    DL_REQUIRE(s && s->s, "invalid argument");
+    return guarded([&] {
+        set_device(s->ctx);
+        dl::session_release(*s->s, instance);
+    });
+}
+
+DL_API dl_status dl_session_memory(const dl_session *s, int64_t *device_bytes, int64_t *active) {
+    DL_REQUIRE(s && s->s, "invalid argument");
+    if (device_bytes) *device_bytes = (int64_t) dl::session_device_bytes(*s->s);
+    if (active) *active = (int64_t) dl::session_active(*s->s);
+    return DL_OK;
+}
+
+DL_API dl_status dl_session_destroy(dl_session *s) {
+    if (!s) return DL_OK;
+    if (s->s) {
+        cudaSetDevice(s->ctx->c.device);
+        dl::session_destroy(s->s);
+    }
+    delete s;
+    return DL_OK;
+}
+
+DL_API dl_status dl_run_batch(dl_context *ctx, int32_t program, const int32_t *const *edges, const int64_t *rows,
+                              int64_t count, int32_t edges_on_device, const dl_options *opts, dl_session **out) {
+    DL_REQUIRE(ctx && out && count >= 0 && (count == 0 || (edges && rows)), "invalid argument");
+    for (int64_t i = 0; i < count; ++i)
+        DL_REQUIRE(rows[i] >= 0 && rows[i] <= (int64_t) 0x7FFFFFFF && (edges[i] || rows[i] == 0),
+                   "invalid edge set");
+    *out = nullptr;
+    u64 nodes = 0;  // upper bound on distinct nodes: two per edge row
+    for (int64_t i = 0; i < count; ++i) nodes += 2 * (u64) rows[i];
+    if (program == DL_PROGRAM_WCC || nodes == 0 || nodes >= (1ull << 30)) nodes = 0;
+    dl_session *s = nullptr;
+    dl_status st = dl_session_create(ctx, program, opts, (int64_t) nodes, &s);
+    if (st != DL_OK) return st;
+    st = guarded([&] {
+        set_device(ctx);
+        for (int64_t i = 0; i < count; ++i) dl::session_admit(*s->s, edges[i], (u64) rows[i], edges_on_device != 0);
+        while (dl::session_step(*s->s) > 0) {
+        }
+        dl::session_fold_profile(*s->s, ctx->c);
+    });
+    if (st != DL_OK) {
+        dl_session_destroy(s);
+        return st;
+    }
+    *out = s;
     return DL_OK;
 }
 

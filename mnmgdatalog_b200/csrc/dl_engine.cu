@@ -18,19 +18,11 @@
 #include "dl_join.cuh"
 #include "dl_scan.cuh"
 #include "dl_engine.h"
+#include "dl_engine_detail.h"
 
 namespace dl {
-namespace {
+namespace detail {
 
-constexpr int T256 = 256;
-
-inline unsigned grid_for(u64 n, int threads, const Context &ctx, int per_sm = 16) {
-    u64 g = (n + threads - 1) / threads;
-    const u64 cap = (u64) ctx.sm_count * per_sm;
-    if (g > cap) g = cap;
-    if (g == 0) g = 1;
-    return (unsigned) g;
-}
 
 #define GRID_STRIDE(i, n) for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (u64) gridDim.x * blockDim.x)
 
@@ -152,41 +144,7 @@ __global__ void unpack_labels_kernel(const u32 *__restrict__ label, u32 n, const
     GRID_STRIDE(u, (u64) n) out[u] = ids[label[u]];
 }
 
-// Device-time accounting per phase (the reference's CSV breakdown).
-struct PhaseTimer {
-    Context &ctx;
-    bool on;
-    std::vector<std::pair<int, cudaEvent_t>> marks;
-    explicit PhaseTimer(Context &c, bool enabled) : ctx(c), on(enabled) {}
-    ~PhaseTimer() {
-        for (auto &m : marks) cudaEventDestroy(m.second);
-    }
-    void mark(int phase) {  // a new phase starts now
-        if (!on) return;
-        cudaEvent_t e;
-        DL_CUDA(cudaEventCreate(&e));
-        DL_CUDA(cudaEventRecord(e, ctx.stream));
-        marks.emplace_back(phase, e);
-    }
-    void finish(double out[5]) {
-        for (int i = 0; i < 5; ++i) out[i] = 0;
-        if (!on || marks.size() < 2) return;
-        DL_CUDA(cudaEventSynchronize(marks.back().second));
-        for (size_t i = 0; i + 1 < marks.size(); ++i) {
-            float ms = 0;
-            DL_CUDA(cudaEventElapsedTime(&ms, marks[i].second, marks[i + 1].second));
-            out[marks[i].first] += ms * 1e-3;
-        }
-    }
-};
-enum { PH_INIT = 0, PH_JOIN = 1, PH_DEDUP = 2, PH_MERGE = 3, PH_FINAL = 4 };
 
-struct Graph {
-    u32 n_ids = 0;
-    int bits = 1;
-    int32_t *ids = nullptr;
-    Csr csr;
-};
 
 int bits_for(u64 n) {
     int b = 1;
@@ -323,14 +281,6 @@ void adopt_ids(Context &ctx, Run &r, const Graph &g) {
 // sparse join output is checked against the large run by binary probes and
 // only the small run is rewritten, and the small run is merged into the large
 // one when it reaches 1/4 of it. The iteration's delta is the same set.
-struct FullSet {
-    int cur = 0;
-    u64 nbig = 0;
-    int scur = 0;
-    u64 nsmall = 0;
-    u64 ns = 0;
-    bool sample_ok = false;
-};
 
 // Measured on B200: a binary probe costs ~50 ps per J word, the fused
 // streaming step ~13 ps per word of (large run + J), so probing wins while
@@ -407,7 +357,9 @@ void settle(Context &ctx, FullSet &F) {
     F.nsmall = 0;
 }
 
-}  // namespace
+}  // namespace detail
+
+using namespace detail;
 
 // ---------------------------------------------------------------------------
 // TC (tc.cu:42-423): path stored reversed as (z, x) keyed by z; edges keyed by

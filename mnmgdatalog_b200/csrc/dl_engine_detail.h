@@ -1,0 +1,78 @@
+// Engine helpers shared by the single-run drivers (dl_engine.cu) and the
+// multi-instance session (dl_session.cu).
+#pragma once
+
+#include "dl_internal.h"
+
+namespace dl {
+namespace detail {
+
+constexpr int T256 = 256;
+
+inline unsigned grid_for(u64 n, int threads, const Context &ctx, int per_sm = 16) {
+    u64 g = (n + threads - 1) / threads;
+    const u64 cap = (u64) ctx.sm_count * per_sm;
+    if (g > cap) g = cap;
+    if (g == 0) g = 1;
+    return (unsigned) g;
+}
+
+// Device-time accounting per phase (the reference's CSV breakdown).
+struct PhaseTimer {
+    Context &ctx;
+    bool on;
+    std::vector<std::pair<int, cudaEvent_t>> marks;
+    explicit PhaseTimer(Context &c, bool enabled) : ctx(c), on(enabled) {}
+    ~PhaseTimer() {
+        for (auto &m : marks) cudaEventDestroy(m.second);
+    }
+    void mark(int phase) {  // a new phase starts now
+        if (!on) return;
+        cudaEvent_t e;
+        DL_CUDA(cudaEventCreate(&e));
+        DL_CUDA(cudaEventRecord(e, ctx.stream));
+        marks.emplace_back(phase, e);
+    }
+    void finish(double out[5]) {
+        for (int i = 0; i < 5; ++i) out[i] = 0;
+        if (!on || marks.size() < 2) return;
+        DL_CUDA(cudaEventSynchronize(marks.back().second));
+        for (size_t i = 0; i + 1 < marks.size(); ++i) {
+            float ms = 0;
+            DL_CUDA(cudaEventElapsedTime(&ms, marks[i].second, marks[i + 1].second));
+            out[marks[i].first] += ms * 1e-3;
+        }
+    }
+};
+enum { PH_INIT = 0, PH_JOIN = 1, PH_DEDUP = 2, PH_MERGE = 3, PH_FINAL = 4 };
+
+struct Graph {
+    u32 n_ids = 0;
+    int bits = 1;
+    int32_t *ids = nullptr;
+    Csr csr;
+};
+
+struct FullSet {
+    int cur = 0;
+    u64 nbig = 0;
+    int scur = 0;
+    u64 nsmall = 0;
+    u64 ns = 0;
+    bool sample_ok = false;
+};
+
+
+int bits_for(u64 n);
+const int32_t *stage_input(Context &ctx, const int32_t *rows, u64 n, bool on_device);
+void rank_nodes(Context &ctx, const int32_t *rows, u64 n, Graph &g);
+u64 *sort_unique_into(Context &ctx, DevBuf &buf, DevBuf &alt, u64 n, int key_bits, u64 &n_out);
+DevBuf &holder(Workspace &ws, const u64 *p);
+DevBuf &other(Workspace &ws, const u64 *p);
+u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, EmitKind kind, u64 &n_j,
+                   u64 *self_pairs, PhaseTimer &pt);
+u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta);
+void settle(Context &ctx, FullSet &F);
+
+}  // namespace detail
+}  // namespace dl

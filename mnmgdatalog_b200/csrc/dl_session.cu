@@ -1,0 +1,815 @@
+// Multi-instance fixpoint session: the batched and served forms.
+//
+// Many independent queries of one program run as ONE union fixpoint. Every
+// admitted instance gets its own contiguous range of node ranks, so its
+// tuples never meet another instance's: joins, sorts, the set difference and
+// the merge of one iteration process every active instance at once, and the
+// per-iteration launch and synchronisation cost is paid once for all of them.
+// Instances are admitted at any iteration boundary (continuous batching):
+// their edges are appended to the union's offset table (their ranks are above
+// every rank in use, so the table stays sorted) and their initial delta joins
+// the next iteration. Each instance keeps its own iteration count and delta
+// sequence (a per-instance histogram of every iteration's delta) and leaves
+// the union when it reaches its own fixpoint -- for WCC with the reference's
+// stop rule an instance is frozen (its delta entries dropped) at the iteration
+// where that rule fires, exactly where the reference program would stop.
+// Results are bit-exact with running each query alone.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+
+#include "dl_engine_detail.h"
+#include "dl_join.cuh"
+#include "dl_scan.cuh"
+#include "dl_session.h"
+
+namespace dl {
+namespace {
+
+using namespace detail;
+
+#define GRID_STRIDE(i, n) \
+    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (u64) gridDim.x * blockDim.x)
+
+// Rows (a, b) of one instance -> fwd (rank a, rank b) / rev (rank b, rank a)
+// words over union ranks (instance ranks start at `base`).
+__global__ void session_pack_kernel(const int32_t *__restrict__ rows, u64 n, const int32_t *__restrict__ ids, u32 n_ids,
+                                    u64 base, int bits, u64 *__restrict__ fwd, u64 *__restrict__ rev) {
+    GRID_STRIDE(i, n) {
+        const int32_t a = rows[2 * i], b = rows[2 * i + 1];
+        u32 lo = 0, hi = n_ids;
+        while (lo < hi) {
+            const u32 m = (lo + hi) >> 1;
+            if (ids[m] < a) lo = m + 1;
+            else hi = m;
+        }
+        const u64 ra = base + lo;
+        lo = 0;
+        hi = n_ids;
+        while (lo < hi) {
+            const u32 m = (lo + hi) >> 1;
+            if (ids[m] < b) lo = m + 1;
+            else hi = m;
+        }
+        const u64 rb = base + lo;
+        if (fwd) fwd[i] = (ra << bits) | rb;
+        if (rev) rev[i] = (rb << bits) | ra;
+    }
+}
+
+// Appends one instance's sorted words to the union offset table:
+// off[r] = base + (first word with key >= r) for r in [lo, hi].
+__global__ void session_csr_kernel(const u64 *__restrict__ w, u64 n, int bits, u64 lo, u64 hi, u64 base,
+                                   u32 *__restrict__ off, u32 *__restrict__ val) {
+    GRID_STRIDE(k, hi - lo + 1) {
+        const u64 target = (lo + k) << bits;
+        u64 l = 0, h = n;
+        while (l < h) {
+            const u64 m = (l + h) >> 1;
+            if (w[m] < target) l = m + 1;
+            else h = m;
+        }
+        off[lo + k] = (u32) (base + l);
+    }
+    const u64 mask = (1ull << bits) - 1;
+    GRID_STRIDE(i, n) val[base + i] = (u32) (w[i] & mask);
+}
+
+// Instance index of a rank: last active instance whose first rank <= r.
+__device__ __forceinline__ u32 instance_of(const u64 *__restrict__ lo, u32 n, u64 r) {
+    u32 a = 0, b = n;
+    while (a < b) {
+        const u32 m = (a + b) >> 1;
+        if (lo[m] <= r) a = m + 1;
+        else b = m;
+    }
+    return a - 1;
+}
+
+// Per-instance count of delta words; the rank is word >> shift.
+__global__ void session_hist_kernel(const u64 *__restrict__ d, u64 n, int shift, const u64 *__restrict__ lo, u32 ninst,
+                                    unsigned long long *__restrict__ cnt) {
+    extern __shared__ u32 sh[];
+    const bool smem = ninst <= 8192;
+    if (smem)
+        for (u32 i = threadIdx.x; i < ninst; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    GRID_STRIDE(i, n) {
+        const u32 k = instance_of(lo, ninst, d[i] >> shift);
+        if (k >= ninst) continue;  // below every active range: not counted
+        if (smem) atomicAdd(&sh[k], 1u);
+        else atomicAdd(&cnt[k], 1ull);
+    }
+    __syncthreads();
+    if (smem)
+        for (u32 i = threadIdx.x; i < ninst; i += blockDim.x)
+            if (sh[i]) atomicAdd(&cnt[i], (unsigned long long) sh[i]);
+}
+
+// [first, end) of the words with key rank in [rlo, rhi) of a sorted run.
+__global__ void session_bounds_kernel(const u64 *__restrict__ w, u64 n, u64 klo, u64 khi, u64 *__restrict__ out) {
+    if (threadIdx.x < 2) {
+        const u64 target = threadIdx.x == 0 ? klo : khi;
+        u64 l = 0, h = n;
+        while (l < h) {
+            const u64 m = (l + h) >> 1;
+            if (w[m] < target) l = m + 1;
+            else h = m;
+        }
+        out[threadIdx.x] = l;
+    }
+}
+
+__global__ void session_label_init_kernel(u32 *__restrict__ label, u32 *__restrict__ flag, u64 lo, u64 hi,
+                                          u64 *__restrict__ delta) {
+    GRID_STRIDE(i, hi - lo) {
+        const u64 r = lo + i;
+        label[r] = (u32) r;
+        flag[r] = 0;
+        delta[i] = (r << 32) | r;
+    }
+}
+
+__global__ void session_next_delta_kernel(const u32 *__restrict__ nodes, u64 count, const u32 *__restrict__ label,
+                                          u32 *__restrict__ flag, u64 *__restrict__ delta) {
+    GRID_STRIDE(i, count) {
+        const u32 v = nodes[i];
+        delta[i] = ((u64) v << 32) | label[v];
+        flag[v] = 0;
+    }
+}
+
+// Components of one instance: counts of the labels of ranks [lo, hi).
+__global__ void session_wcc_count_kernel(const u32 *__restrict__ label, u64 lo, u64 hi, u32 *__restrict__ cnt) {
+    GRID_STRIDE(i, hi - lo) atomicAdd(&cnt[label[lo + i] - lo], 1u);
+}
+
+struct NonZero {
+    const u32 *c;
+    __device__ __forceinline__ u64 degree(u64 i) const { return c[i] != 0u; }
+};
+
+__global__ void session_wcc_comp_kernel(const u32 *__restrict__ cnt, u64 n, const u64 *__restrict__ pos,
+                                        u32 *__restrict__ comp, unsigned long long *__restrict__ largest) {
+    GRID_STRIDE(c, n) {
+        const u32 k = cnt[c];
+        if (k) {
+            comp[pos[c]] = (u32) c;
+            atomicMax(largest, (unsigned long long) k);
+        }
+    }
+}
+
+// Keep delta words whose instance is still active (freezing finished ones).
+struct KeepActive {
+    const u64 *lo;
+    const uint8_t *live;
+    u32 n;
+    int shift;
+    __device__ bool operator()(u64 cur, u64, bool) const {
+        const u32 k = instance_of(lo, n, cur >> shift);
+        return k < n && live[k] != 0;
+    }
+};
+
+template <bool KeyFirst>
+__global__ void session_unpack_kernel(const u64 *__restrict__ w, u64 n, int bits, u64 base,
+                                      const int32_t *__restrict__ ids, int32_t *__restrict__ out) {
+    const u64 mask = (1ull << bits) - 1;
+    GRID_STRIDE(i, n) {
+        const u64 x = w[i];
+        const int32_t hi = ids[(x >> bits) - base], lo = ids[(x & mask) - base];
+        int2 r;
+        r.x = KeyFirst ? hi : lo;
+        r.y = KeyFirst ? lo : hi;
+        reinterpret_cast<int2 *>(out)[i] = r;
+    }
+}
+
+__global__ void session_unpack_comp_kernel(const u32 *__restrict__ comp, u64 n, const int32_t *__restrict__ ids,
+                                           int32_t *__restrict__ out) {
+    GRID_STRIDE(i, n) {
+        int2 r;
+        r.x = ids[comp[i]];
+        r.y = 0;
+        reinterpret_cast<int2 *>(out)[i] = r;
+    }
+}
+
+// labels: union label rank of each local node; ids indexed by local rank.
+__global__ void session_unpack_labels_kernel(const u32 *__restrict__ label, u64 lo, u64 n,
+                                             const int32_t *__restrict__ ids, int32_t *__restrict__ out) {
+    GRID_STRIDE(i, n) out[i] = ids[label[i] - lo];
+}
+
+// Keeps the words whose instance (rank = word >> shift) is live.
+template <class Keep>
+u64 session_select(Context &ctx, u64 *buf, u64 n, Keep keep, int slot) {
+    if (n == 0) return 0;
+    const u64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    u64 *lb = ctx.lookback_words(tiles);
+    u32 *ctr = ctx.tile_counter(slot);
+    u64 *cnt = &ctx.ctrl->scalar[28];
+    DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(u32), ctx.stream));
+    DL_LAUNCH(ctx, K_SELECT, 16.0 * n,
+              select_kernel<Keep><<<(unsigned) tiles, SCAN_THREADS, 0, ctx.stream>>>(
+                  buf, n, buf, keep, lb, ctr, ctx.next_epoch(), &ctx.ctrl->err, cnt));
+    DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 4, cnt, sizeof(u64), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    return ctx.host_scalars[4];
+}
+
+// Grows a buffer keeping its first `keep` bytes.
+void grow_keep(Context &ctx, DevBuf &b, size_t bytes, size_t keep) {
+    if (b.p && b.cap >= bytes) return;
+    DevBuf nb;
+    nb.reserve(std::max(bytes, b.cap * 3 / 2));
+    if (keep && b.p) DL_CUDA(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice, ctx.stream));
+    ctx.sync();
+    b.release();
+    b = nb;
+}
+
+}  // namespace
+
+struct SessionImpl {
+    Context ctx;  // private workspace; shares the caller's stream
+    int program = DL_PROGRAM_TC;
+    dl_options opt{};
+    int bits = 30;
+    u64 rank_cap = 0;
+    u64 next_rank = 0;
+    DevBuf off, val;  // union offset table over ranks, values
+    u64 n_vals = 0;
+    FullSet F;
+    u64 dead = 0;  // words of finished instances still in the full runs
+    DevBuf delta;  // union delta (probe of the next iteration)
+    u64 n_delta = 0;
+    DevBuf label, flag, nextl;  // WCC
+    DevBuf inst_lo, inst_hi;    // device copies of the active instances' rank ranges
+    DevBuf counts;              // per active instance delta counts
+    DevBuf live;                // per active instance flag (WCC freezing)
+    std::vector<SessionInstance> inst;
+    std::vector<i64> active;    // instance ids in rank order
+    std::vector<i64> finished;  // finished since the last poll
+    bool inst_dirty = true;
+};
+
+namespace {
+
+Graph union_graph(SessionImpl &s) {
+    Graph g;
+    g.n_ids = (u32) s.next_rank;
+    g.bits = s.bits;
+    g.csr.off = s.off.as<u32>();
+    g.csr.val = s.val.as<u32>();
+    g.csr.n_keys = (u32) s.next_rank;
+    g.csr.n_vals = s.n_vals;
+    return g;
+}
+
+// Inserts the words of a brand-new key range into the full relation.
+void full_insert_new(SessionImpl &s, const u64 *w, u64 n) {
+    Context &ctx = s.ctx;
+    Workspace &ws = ctx.ws;
+    FullSet &F = s.F;
+    if (n == 0) return;
+    ctx.reserve(ws.small[1 - F.scur], (F.nsmall + n) * 8);
+    merge_words(ctx, ws.small[F.scur].as<u64>(), F.nsmall, w, n, ws.small[1 - F.scur].as<u64>(), Codec::Raw);
+    F.scur = 1 - F.scur;
+    F.nsmall += n;
+    if (F.nsmall * 4 >= F.nbig) {
+        ctx.reserve(ws.full[1 - F.cur], (F.nbig + F.nsmall) * 8);
+        merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.small[F.scur].as<u64>(), F.nsmall,
+                    ws.full[1 - F.cur].as<u64>(), Codec::Raw);
+        F.cur = 1 - F.cur;
+        F.nbig += F.nsmall;
+        F.nsmall = 0;
+        F.sample_ok = false;
+    }
+}
+
+void delta_append(SessionImpl &s, const u64 *w, u64 n) {
+    if (n == 0) return;
+    grow_keep(s.ctx, s.delta, (s.n_delta + n) * 8, s.n_delta * 8);
+    DL_CUDA(cudaMemcpyAsync(s.delta.as<u64>() + s.n_delta, w, n * 8, cudaMemcpyDeviceToDevice, s.ctx.stream));
+    s.n_delta += n;
+}
+
+void upload_active(SessionImpl &s) {
+    if (!s.inst_dirty) return;
+    const u64 na = s.active.size();
+    std::vector<u64> lo(std::max<u64>(na, 1)), hi(std::max<u64>(na, 1));
+    for (u64 i = 0; i < na; ++i) {
+        lo[i] = s.inst[s.active[i]].rank_lo;
+        hi[i] = s.inst[s.active[i]].rank_hi;
+    }
+    s.ctx.reserve(s.inst_lo, lo.size() * 8);
+    s.ctx.reserve(s.inst_hi, hi.size() * 8);
+    DL_CUDA(cudaMemcpyAsync(s.inst_lo.p, lo.data(), na * 8, cudaMemcpyHostToDevice, s.ctx.stream));
+    DL_CUDA(cudaMemcpyAsync(s.inst_hi.p, hi.data(), na * 8, cudaMemcpyHostToDevice, s.ctx.stream));
+    s.ctx.sync();  // lo/hi are host temporaries
+    s.inst_dirty = false;
+}
+
+// Per-active-instance counts of the words in d (rank = word >> shift).
+std::vector<u64> delta_counts(SessionImpl &s, const u64 *d, u64 n, int shift) {
+    Context &ctx = s.ctx;
+    const u64 na = s.active.size();
+    std::vector<u64> c(na, 0);
+    if (na == 0) return c;
+    if (n == 0) return c;
+    upload_active(s);
+    ctx.reserve(s.counts, na * 8);
+    DL_CUDA(cudaMemsetAsync(s.counts.p, 0, na * 8, ctx.stream));
+    const unsigned smem = na <= 8192 ? (unsigned) (na * 4) : 0u;
+    DL_LAUNCH(ctx, K_PREP, 8.0 * n,
+              session_hist_kernel<<<grid_for(n, 256, ctx, 8), 256, smem, ctx.stream>>>(
+                  d, n, shift, s.inst_lo.as<u64>(), (u32) na, (unsigned long long *) s.counts.p));
+    DL_CUDA(cudaMemcpyAsync(c.data(), s.counts.p, na * 8, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    return c;
+}
+
+// Sorted words of one TC/SG instance out of both full runs.
+void extract_words(SessionImpl &s, SessionInstance &in) {
+    Context &ctx = s.ctx;
+    Workspace &ws = ctx.ws;
+    const u64 klo = in.rank_lo << s.bits, khi = in.rank_hi << s.bits;
+    u64 *bnd = &ctx.ctrl->scalar[20];
+    DL_LAUNCH(ctx, K_PREP, 0,
+              session_bounds_kernel<<<1, 32, 0, ctx.stream>>>(ws.full[s.F.cur].as<u64>(), s.F.nbig, klo, khi, bnd));
+    DL_LAUNCH(ctx, K_PREP, 0,
+              session_bounds_kernel<<<1, 32, 0, ctx.stream>>>(ws.small[s.F.scur].as<u64>(), s.F.nsmall, klo, khi,
+                                                               bnd + 2));
+    DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 8, bnd, 32, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    const u64 *hb = ctx.host_scalars + 8;
+    const u64 a0 = hb[0], na = hb[1] - hb[0], b0 = hb[2], nb = hb[3] - hb[2];
+    in.n_result = na + nb;
+    ctx.reserve(in.result, std::max<u64>(in.n_result, 1) * 8);
+    if (in.n_result)
+        merge_words(ctx, ws.full[s.F.cur].as<u64>() + a0, na, ws.small[s.F.scur].as<u64>() + b0, nb,
+                    in.result.as<u64>(), Codec::Raw);
+    s.dead += in.n_result;
+}
+
+void extract_components(SessionImpl &s, SessionInstance &in) {
+    Context &ctx = s.ctx;
+    const u64 n = in.rank_hi - in.rank_lo;
+    DevBuf cnt, pos;
+    ctx.reserve(cnt, std::max<u64>(n, 1) * 4);
+    ctx.reserve(pos, std::max<u64>(n, 1) * 8);
+    DL_CUDA(cudaMemsetAsync(cnt.p, 0, n * 4, ctx.stream));
+    DL_LAUNCH(ctx, K_PREP, 0,
+              session_wcc_count_kernel<<<grid_for(n, 256, ctx, 8), 256, 0, ctx.stream>>>(s.label.as<u32>(), in.rank_lo,
+                                                                                         in.rank_hi, cnt.as<u32>()));
+    const u64 nc = count_matches(ctx, NonZero{cnt.as<u32>()}, n, pos.as<u64>());
+    u64 *largest = &ctx.ctrl->scalar[24];
+    DL_CUDA(cudaMemsetAsync(largest, 0, 8, ctx.stream));
+    ctx.reserve(in.result, std::max<u64>(nc, 1) * 4);
+    DL_LAUNCH(ctx, K_PREP, 0,
+              session_wcc_comp_kernel<<<grid_for(n, 256, ctx, 8), 256, 0, ctx.stream>>>(
+                  cnt.as<u32>(), n, pos.as<u64>(), in.result.as<u32>(), (unsigned long long *) largest));
+    ctx.reserve(in.labels, std::max<u64>(n, 1) * 4);
+    DL_CUDA(cudaMemcpyAsync(in.labels.p, s.label.as<u32>() + in.rank_lo, n * 4, cudaMemcpyDeviceToDevice, ctx.stream));
+    DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 12, largest, 8, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    in.n_result = nc;
+    in.largest = (i64) ctx.host_scalars[12];
+    ctx.give_back(cnt);
+    ctx.give_back(pos);
+}
+
+void mark_done(SessionImpl &s, SessionInstance &in) {
+    in.active = false;
+    in.done = true;
+    s.finished.push_back(in.id);
+}
+
+void finish(SessionImpl &s, i64 id) {
+    SessionInstance &in = s.inst[id];
+    if (s.program == DL_PROGRAM_WCC) extract_components(s, in);
+    else extract_words(s, in);
+    mark_done(s, in);
+}
+
+// Drops the union state once no instance is active: ranks, offsets and the
+// full relation start again from zero (results live with their instances).
+void reset_if_idle(SessionImpl &s) {
+    if (!s.active.empty()) return;
+    s.next_rank = 0;
+    s.n_vals = 0;
+    s.F = FullSet();
+    s.dead = 0;
+    s.n_delta = 0;
+    s.inst_dirty = true;
+}
+
+// Words whose key rank lies in an active instance's range.
+struct KeepLive {
+    const u64 *lo, *hi;
+    u32 n;
+    int shift;
+    __device__ bool operator()(u64 cur, u64, bool) const {
+        const u64 r = cur >> shift;
+        const u32 k = instance_of(lo, n, r);
+        return k < n && r < hi[k];
+    }
+};
+
+// Removes the words of finished instances from the full runs once they are
+// at least half of the full relation.
+void maybe_compact(SessionImpl &s) {
+    if (s.program == DL_PROGRAM_WCC || s.active.empty()) return;
+    const u64 total = s.F.nbig + s.F.nsmall;
+    if (s.dead == 0 || s.dead * 2 < total) return;
+    Context &ctx = s.ctx;
+    Workspace &ws = ctx.ws;
+    upload_active(s);
+    KeepLive keep{s.inst_lo.as<u64>(), s.inst_hi.as<u64>(), (u32) s.active.size(), s.bits};
+    s.F.nbig = session_select(ctx, ws.full[s.F.cur].as<u64>(), s.F.nbig, keep, 60);
+    s.F.nsmall = session_select(ctx, ws.small[s.F.scur].as<u64>(), s.F.nsmall, keep, 60);
+    s.F.sample_ok = false;
+    s.dead = 0;
+}
+
+void retire(SessionImpl &s, const std::vector<i64> &done, const std::vector<i64> &still) {
+    for (i64 id : done) finish(s, id);
+    if (still.size() != s.active.size()) {
+        s.active = still;
+        s.inst_dirty = true;
+    }
+    reset_if_idle(s);
+}
+
+u64 wcc_step(SessionImpl &s) {
+    Context &ctx = s.ctx;
+    Workspace &ws = ctx.ws;
+    ctx.reserve(ws.offsets, std::max<u64>(s.n_delta, 1) * 8);
+    u32 *next_count = reinterpret_cast<u32 *>(&ctx.ctrl->scalar[32]);
+    DL_CUDA(cudaMemsetAsync(next_count, 0, 4, ctx.stream));
+    Graph g = union_graph(s);
+    WccSrc src{g.csr.off, g.csr.val, s.delta.as<u64>(), s.label.as<u32>(), s.flag.as<u32>(), s.nextl.as<u32>(),
+               next_count};
+    const u64 total = count_matches(ctx, src, s.n_delta, ws.offsets.as<u64>());  // wcc.cu:255-300
+    if (total) emit_matches(ctx, src, s.n_delta, ws.offsets.as<u64>(), total, nullptr, nullptr, 0, nullptr);
+    DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 6, next_count, 4, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    const u64 nn = *reinterpret_cast<u32 *>(ctx.host_scalars + 6);
+    grow_keep(ctx, s.delta, std::max<u64>(nn, 1) * 8, 0);  // the emit has read the old delta
+    if (nn)  // rebuild the delta from the appended nodes
+        DL_LAUNCH(ctx, K_PREP, 0,
+                  session_next_delta_kernel<<<grid_for(nn, 256, ctx, 16), 256, 0, ctx.stream>>>(
+                      s.nextl.as<u32>(), nn, s.label.as<u32>(), s.flag.as<u32>(), s.delta.as<u64>()));
+    s.n_delta = nn;
+    const std::vector<u64> c = delta_counts(s, s.delta.as<u64>(), nn, 32);
+    std::vector<i64> still, done;
+    std::vector<uint8_t> live(s.active.size(), 1);
+    bool frozen_rows = false;
+    for (u64 k = 0; k < s.active.size(); ++k) {
+        SessionInstance &in = s.inst[s.active[k]];
+        const i64 cnt = (i64) c[k];
+        in.deltas.push_back(cnt);
+        bool stop = s.opt.wcc_stop == DL_WCC_STOP_FIXPOINT ? cnt == 0 : cnt == in.prev_delta;  // wcc.cu:366-383
+        in.prev_delta = cnt;
+        if (!stop && s.opt.max_iterations > 0 && (int) in.deltas.size() >= s.opt.max_iterations) stop = true;
+        if (stop) {
+            live[k] = 0;
+            frozen_rows |= cnt != 0;
+            done.push_back(s.active[k]);
+        } else {
+            still.push_back(s.active[k]);
+        }
+    }
+    if (frozen_rows) {  // an instance stopped with a non-empty delta: drop its rows
+        ctx.reserve(s.live, live.size());
+        DL_CUDA(cudaMemcpyAsync(s.live.p, live.data(), live.size(), cudaMemcpyHostToDevice, ctx.stream));
+        KeepActive keep{s.inst_lo.as<u64>(), s.live.as<uint8_t>(), (u32) s.active.size(), 32};
+        s.n_delta = session_select(ctx, s.delta.as<u64>(), s.n_delta, keep, 61);  // syncs: `live` may go
+    }
+    retire(s, done, still);
+    return s.active.size();
+}
+
+u64 fixpoint_step(SessionImpl &s) {
+    Context &ctx = s.ctx;
+    Workspace &ws = ctx.ws;
+    Graph g = union_graph(s);
+    PhaseTimer pt(ctx, false);
+    u64 nnew = 0;
+    u64 *dnew = nullptr;
+    if (s.program == DL_PROGRAM_TC) {  // tc.cu:216-314
+        u64 nj = 0;
+        u64 *j = join_and_sort(ctx, g, s.delta.as<u64>(), s.n_delta, EmitKind::ZV, nj, nullptr, pt);
+        dnew = absorb(ctx, s.F, j, nj, nnew);
+    } else {  // sg.cu:244-390
+        u64 n1 = 0, n2 = 0;
+        u64 *j1 = join_and_sort(ctx, g, s.delta.as<u64>(), s.n_delta, EmitKind::VZ, n1, nullptr, pt);
+        if (n1) n1 = unique_words(ctx, j1, n1, j1);
+        if (n1) {
+            u64 *j2 = join_and_sort(ctx, g, j1, n1, EmitKind::VZ, n2, nullptr, pt);
+            dnew = absorb(ctx, s.F, j2, n2, nnew);
+        }
+    }
+    // the new delta sits in one of the join buffers: trade it for the old delta's buffer
+    if (nnew) std::swap(s.delta, holder(ws, dnew));
+    s.n_delta = nnew;
+    const std::vector<u64> c = delta_counts(s, s.delta.as<u64>(), nnew, s.bits);
+    std::vector<i64> still, done;
+    for (u64 k = 0; k < s.active.size(); ++k) {
+        SessionInstance &in = s.inst[s.active[k]];
+        in.deltas.push_back((i64) c[k]);
+        bool stop = c[k] == 0;  // |full| unchanged
+        if (!stop && s.opt.max_iterations > 0 && (int) in.deltas.size() >= s.opt.max_iterations) stop = true;
+        (stop ? done : still).push_back(s.active[k]);
+    }
+    if (!done.empty() && nnew && still.size() < s.active.size()) {
+        // an instance stopped by max_iterations keeps rows in the delta: drop them
+        bool rows_left = false;
+        for (u64 k = 0; k < s.active.size(); ++k)
+            if (c[k] && std::find(done.begin(), done.end(), s.active[k]) != done.end()) rows_left = true;
+        if (rows_left) {
+            std::vector<uint8_t> live(s.active.size(), 1);
+            for (u64 k = 0; k < s.active.size(); ++k)
+                if (std::find(done.begin(), done.end(), s.active[k]) != done.end()) live[k] = 0;
+            ctx.reserve(s.live, live.size());
+            DL_CUDA(cudaMemcpyAsync(s.live.p, live.data(), live.size(), cudaMemcpyHostToDevice, ctx.stream));
+            KeepActive keep{s.inst_lo.as<u64>(), s.live.as<uint8_t>(), (u32) s.active.size(), s.bits};
+            s.n_delta = session_select(ctx, s.delta.as<u64>(), s.n_delta, keep, 61);
+        }
+    }
+    retire(s, done, still);
+    maybe_compact(s);
+    return s.active.size();
+}
+
+}  // namespace
+
+SessionImpl *session_create(Context &parent, int program, const dl_options &opt, u64 max_nodes) {
+    if (program != DL_PROGRAM_TC && program != DL_PROGRAM_SG && program != DL_PROGRAM_WCC)
+        throw Error(DL_ERR_INVALID_ARGUMENT, "sessions run TC, SG or WCC");
+    auto s = std::make_unique<SessionImpl>();
+    s->program = program;
+    s->opt = opt;
+    if (program == DL_PROGRAM_WCC) {
+        // WCC words are (rank << 32 | label rank)
+        s->bits = 32;
+        s->rank_cap = 0xFFFFFFFFull;
+    } else {
+        // TC/SG words hold two ranks; fewer bits mean fewer radix passes
+        s->bits = max_nodes ? std::max(1, bits_for(max_nodes)) : 30;
+        if (s->bits > 31) throw Error(DL_ERR_INVALID_ARGUMENT, "max_nodes above 2^31");
+        s->rank_cap = 1ull << s->bits;
+    }
+    Context &c = s->ctx;
+    c.device = parent.device;
+    c.stream = parent.stream;
+    c.sm_count = parent.sm_count;
+    c.prof_on = parent.prof_on;
+    void *p = nullptr;
+    DL_CUDA(cudaMalloc(&p, sizeof(Ctrl)));
+    c.ctrl = (Ctrl *) p;
+    DL_CUDA(cudaMemset(p, 0, sizeof(Ctrl)));
+    DL_CUDA(cudaMallocHost((void **) &c.host_scalars, 64 * sizeof(u64)));
+    std::memset(c.host_scalars, 0, 64 * sizeof(u64));
+    return s.release();
+}
+
+void session_destroy(SessionImpl *s) {
+    if (!s) return;
+    Context &c = s->ctx;
+    cudaStreamSynchronize(c.stream);
+    for (auto &in : s->inst) {
+        in.ids.release();
+        in.result.release();
+        in.labels.release();
+    }
+    DevBuf *bufs[] = {&s->off,  &s->val,     &s->delta,   &s->label,  &s->flag,
+                      &s->nextl, &s->inst_lo, &s->inst_hi, &s->counts, &s->live};
+    for (DevBuf *b : bufs) b->release();
+    c.release_all();
+    if (c.ctrl) cudaFree(c.ctrl);
+    if (c.host_scalars) cudaFreeHost(c.host_scalars);
+    delete s;
+}
+
+i64 session_admit(SessionImpl &s, const int32_t *rows_in, u64 n, bool on_device) {
+    Context &ctx = s.ctx;
+    Workspace &ws = ctx.ws;
+    s.inst.emplace_back();
+    SessionInstance &in = s.inst.back();
+    in.id = (i64) s.inst.size() - 1;
+    in.input_rows = (i64) n;
+    in.rank_lo = in.rank_hi = s.next_rank;
+    if (n == 0) {  // the program never enters its loop: zero iterations, empty result
+        mark_done(s, in);
+        return in.id;
+    }
+    try {
+        const int32_t *rows = stage_input(ctx, rows_in, n, on_device);
+        Graph gi;
+        rank_nodes(ctx, rows, n, gi);  // distinct ids of this instance, sorted, in ws.ids
+        const u64 nid = gi.n_ids;
+        if (s.next_rank + nid > s.rank_cap)
+            throw Error(DL_ERR_OVERFLOW, "session node capacity exhausted (" + std::to_string(s.rank_cap) + " ranks)");
+        ctx.reserve(in.ids, nid * 4);
+        DL_CUDA(cudaMemcpyAsync(in.ids.p, gi.ids, nid * 4, cudaMemcpyDeviceToDevice, ctx.stream));
+        in.n_ids = (u32) nid;
+        in.rank_lo = s.next_rank;
+        in.rank_hi = s.next_rank + nid;
+        const bool wcc = s.program == DL_PROGRAM_WCC;
+        const u64 m = wcc ? 2 * n : n;
+        ctx.reserve(ws.w0, m * 8);
+        ctx.reserve(ws.w1, m * 8);
+        ctx.reserve(ws.jbuf[0], n * 8);
+        ctx.reserve(ws.jbuf[1], n * 8);
+        const int bits = s.bits;
+        u64 *fw = ws.w0.as<u64>();
+        u64 *rv = wcc ? fw + n : (s.program == DL_PROGRAM_TC ? ws.jbuf[0].as<u64>() : nullptr);
+        DL_LAUNCH(ctx, K_PREP, 0,
+                  session_pack_kernel<<<grid_for(n, 256, ctx, 16), 256, 0, ctx.stream>>>(rows, n, gi.ids, (u32) nid,
+                                                                                          in.rank_lo, bits, fw, rv));
+        u64 ne;
+        // tc.cu:171-176, sg.cu:150-153, wcc.cu:140-167: deduplicated edges keyed by source
+        u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, m, 2 * bits, ne);
+        if (s.n_vals + ne >= (1ull << 32)) throw Error(DL_ERR_OVERFLOW, "session edge capacity exhausted");
+        grow_keep(ctx, s.off, (in.rank_hi + 1) * 4, (in.rank_lo + 1) * 4);
+        grow_keep(ctx, s.val, (s.n_vals + ne + 1) * 4, s.n_vals * 4);
+        DL_LAUNCH(ctx, K_PREP, 0,
+                  session_csr_kernel<<<grid_for(std::max<u64>(ne, nid + 1), 256, ctx, 16), 256, 0, ctx.stream>>>(
+                      e, ne, bits, in.rank_lo, in.rank_hi, s.n_vals, s.off.as<u32>(), s.val.as<u32>()));
+        s.n_vals += ne;
+        s.next_rank = in.rank_hi;
+        if (s.program == DL_PROGRAM_TC) {
+            u64 nd;
+            u64 *d = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * bits, nd);  // tc.cu:178-189
+            full_insert_new(s, d, nd);
+            delta_append(s, d, nd);
+        } else if (s.program == DL_PROGRAM_SG) {
+            // sg.cu:170-217: base rule of this instance, probing the union table
+            Graph g = union_graph(s);
+            u64 *selfs = &ctx.ctrl->scalar[30];
+            DL_CUDA(cudaMemsetAsync(selfs, 0, 8, ctx.stream));
+            u64 nb = 0;
+            PhaseTimer pt(ctx, false);
+            u64 *b = join_and_sort(ctx, g, e, ne, EmitKind::ZV_NOSELF, nb, selfs, pt);
+            DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 5, selfs, 8, cudaMemcpyDeviceToHost, ctx.stream));
+            ctx.sync();
+            const u64 nv = nb - ctx.host_scalars[5];  // self pairs sorted to the end
+            const u64 nd = nv ? unique_words(ctx, b, nv, b) : 0;
+            full_insert_new(s, b, nd);
+            delta_append(s, b, nd);
+            if (nd == 0) {  // the loop runs once on an empty delta (sg.cu:244-390)
+                in.deltas.push_back(0);
+                in.n_result = 0;
+                mark_done(s, in);
+                return in.id;
+            }
+        } else {  // wcc.cu:211-231: cc(n, n) for every node, all nodes in the first delta
+            grow_keep(ctx, s.label, in.rank_hi * 4, in.rank_lo * 4);
+            grow_keep(ctx, s.flag, in.rank_hi * 4, in.rank_lo * 4);
+            grow_keep(ctx, s.nextl, (in.rank_hi + 1) * 4, 0);
+            grow_keep(ctx, s.delta, (s.n_delta + nid) * 8, s.n_delta * 8);
+            DL_LAUNCH(ctx, K_PREP, 0,
+                      session_label_init_kernel<<<grid_for(nid, 256, ctx, 16), 256, 0, ctx.stream>>>(
+                          s.label.as<u32>(), s.flag.as<u32>(), in.rank_lo, in.rank_hi,
+                          s.delta.as<u64>() + s.n_delta));
+            s.n_delta += nid;
+            in.prev_delta = (i64) nid;
+        }
+        ctx.sync();
+    } catch (...) {
+        // the union tables may hold part of this instance; its ranks are never reused
+        in.done = true;
+        in.released = true;
+        throw;
+    }
+    in.active = true;
+    s.active.push_back(in.id);
+    s.inst_dirty = true;
+    return in.id;
+}
+
+u64 session_step(SessionImpl &s) {
+    if (s.active.empty()) return 0;
+    return s.program == DL_PROGRAM_WCC ? wcc_step(s) : fixpoint_step(s);
+}
+
+u64 session_poll(SessionImpl &s, int64_t *ids, u64 capacity) {
+    const u64 n = std::min<u64>(capacity, s.finished.size());
+    for (u64 i = 0; i < n; ++i) ids[i] = s.finished[i];
+    s.finished.erase(s.finished.begin(), s.finished.begin() + (std::ptrdiff_t) n);
+    return n;
+}
+
+void session_fold_profile(SessionImpl &s, Context &parent) {
+    s.ctx.sync();  // resolves the timed launches
+    for (int k = 0; k < K_COUNT; ++k) {
+        KernelStat &a = parent.kstat[k];
+        KernelStat &b = s.ctx.kstat[k];
+        a.launches += b.launches;
+        a.timed += b.timed;
+        a.seconds += b.seconds;
+        a.bytes += b.bytes;
+        b = KernelStat();
+    }
+    s.ctx.prof_on = parent.prof_on;
+}
+
+const SessionInstance &session_instance(const SessionImpl &s, i64 id) {
+    if (id < 0 || id >= (i64) s.inst.size()) throw Error(DL_ERR_INVALID_ARGUMENT, "unknown instance " + std::to_string(id));
+    return s.inst[id];
+}
+
+void session_info(const SessionImpl &s, i64 id, dl_run_info &info) {
+    const SessionInstance &in = session_instance(s, id);
+    std::memset(&info, 0, sizeof(info));
+    info.program = s.program;
+    info.iterations = (int32_t) in.deltas.size();
+    info.input_rows = in.input_rows;
+    info.output_rows = info.output_tuples = in.done ? (i64) in.n_result : 0;
+    info.largest_component = in.largest;
+    info.nodes = in.n_ids;
+}
+
+static SessionInstance &finished_instance(SessionImpl &s, i64 id) {
+    session_instance(s, id);
+    SessionInstance &in = s.inst[id];
+    if (!in.done) throw Error(DL_ERR_INVALID_ARGUMENT, "instance " + std::to_string(id) + " has not finished");
+    if (in.released) throw Error(DL_ERR_INVALID_ARGUMENT, "instance " + std::to_string(id) + " was released");
+    return in;
+}
+
+void session_copy_output(SessionImpl &s, i64 id, int32_t *dst, u64 capacity, bool on_device) {
+    SessionInstance &in = finished_instance(s, id);
+    Context &ctx = s.ctx;
+    const u64 n = in.n_result;
+    if (capacity < n) throw Error(DL_ERR_INVALID_ARGUMENT, "output capacity too small");
+    if (n == 0) return;
+    DevBuf stage;
+    int32_t *tmp = dst;
+    if (!on_device) {
+        ctx.reserve(stage, n * 8);
+        tmp = stage.as<int32_t>();
+    }
+    const int32_t *ids = in.ids.as<int32_t>();
+    const unsigned g = grid_for(n, 256, ctx, 16);
+    if (s.program == DL_PROGRAM_WCC)
+        DL_LAUNCH(ctx, K_PREP, 0, session_unpack_comp_kernel<<<g, 256, 0, ctx.stream>>>(in.result.as<u32>(), n, ids, tmp));
+    else if (s.program == DL_PROGRAM_SG)
+        DL_LAUNCH(ctx, K_PREP, 0,
+                  session_unpack_kernel<true><<<g, 256, 0, ctx.stream>>>(in.result.as<u64>(), n, s.bits, in.rank_lo,
+                                                                          ids, tmp));
+    else
+        DL_LAUNCH(ctx, K_PREP, 0,
+                  session_unpack_kernel<false><<<g, 256, 0, ctx.stream>>>(in.result.as<u64>(), n, s.bits, in.rank_lo,
+                                                                           ids, tmp));
+    if (!on_device) DL_CUDA(cudaMemcpyAsync(dst, tmp, n * 8, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    ctx.give_back(stage);
+}
+
+void session_copy_labels(SessionImpl &s, i64 id, int32_t *node_ids, int32_t *labels, u64 capacity) {
+    SessionInstance &in = finished_instance(s, id);
+    if (s.program != DL_PROGRAM_WCC) throw Error(DL_ERR_INVALID_ARGUMENT, "labels exist only for WCC sessions");
+    Context &ctx = s.ctx;
+    const u64 n = in.n_ids;
+    if (capacity < n) throw Error(DL_ERR_INVALID_ARGUMENT, "label capacity too small");
+    if (n == 0) return;
+    DevBuf stage;
+    ctx.reserve(stage, n * 4);
+    DL_LAUNCH(ctx, K_PREP, 0,
+              session_unpack_labels_kernel<<<grid_for(n, 256, ctx, 16), 256, 0, ctx.stream>>>(
+                  in.labels.as<u32>(), in.rank_lo, n, in.ids.as<int32_t>(), stage.as<int32_t>()));
+    DL_CUDA(cudaMemcpyAsync(labels, stage.p, n * 4, cudaMemcpyDeviceToHost, ctx.stream));
+    DL_CUDA(cudaMemcpyAsync(node_ids, in.ids.p, n * 4, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    ctx.give_back(stage);
+}
+
+void session_release(SessionImpl &s, i64 id) {
+    SessionInstance &in = finished_instance(s, id);
+    s.ctx.give_back(in.result);
+    s.ctx.give_back(in.labels);
+    s.ctx.give_back(in.ids);
+    in.released = true;
+}
+
+u64 session_device_bytes(const SessionImpl &s) {
+    const Context &c = s.ctx;
+    const Workspace &w = c.ws;
+    u64 b = 0;
+    const DevBuf *bufs[] = {&s.off,     &s.val,       &s.delta,    &s.label,      &s.flag,       &s.nextl,
+                            &w.input,   &w.ids,       &w.w0,       &w.w1,         &w.csr_off,    &w.csr_val,
+                            &w.full[0], &w.full[1],   &w.small[0], &w.small[1],   &w.sample,     &w.jbuf[0],
+                            &w.jbuf[1], &w.offsets,   &c.lookback, &c.radix_part, &c.lbs_splits, &c.sort_hist};
+    for (const DevBuf *x : bufs) b += x->cap;
+    for (const auto &x : c.spares) b += x.cap;
+    for (const auto &in : s.inst) b += in.ids.cap + in.result.cap + in.labels.cap;
+    return b;
+}
+
+u64 session_active(const SessionImpl &s) { return s.active.size(); }
+
+}  // namespace dl

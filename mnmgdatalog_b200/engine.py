@@ -216,6 +216,17 @@ class Engine:
     def single_join(self, rows, **kw) -> RunResult:
         return self.run("single_join", rows, **kw)
 
+    # ---- batched / served forms (mnmgdatalog_b200/session.py) ---------------
+    def session(self, program: str, **kw):
+        """A union session of one program (dl_session_create)."""
+        from .session import Session
+        return Session(self, program, **kw)
+
+    def run_batch(self, program: str, edge_sets, **kw) -> list:
+        """Every edge set as one instance of one union fixpoint (dl_run_batch)."""
+        from .session import run_batch
+        return run_batch(self, program, edge_sets, **kw)
+
     # ---- relational operators (CUDA tensors) -------------------------------
     def sort_unique(self, rel):
         """thrust::sort(set_cmp) + thrust::unique(is_equal), in place; returns
