@@ -239,6 +239,8 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
 
     # dominant kernel class by device time over the timed region
     peak, peak_kind = measured_peak_gbs()
+    host = {k: v for k, v in prof.items() if k.startswith("host_")}
+    prof = {k: v for k, v in prof.items() if not k.startswith("host_")}
     dom_name, dom = max(((k, v) for k, v in prof.items() if v["timed_launches"]), key=lambda kv: kv[1]["seconds"])
     launches = sum(v["launches"] for v in prof.values())
     achieved = dom["bytes"] / dom["seconds"] / 1e9 if dom["seconds"] else 0.0
@@ -251,6 +253,7 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
     kernels = {k: {"launches": v["launches"], "ms": round(1e3 * v["seconds"], 3),
                    "GBps": round(v["bytes"] / v["seconds"] / 1e9, 1) if v["seconds"] else None}
                for k, v in prof.items() if v["launches"]}
+    host_costs = {k: {"calls": v["launches"], "ms": round(1e3 * v["seconds"], 3)} for k, v in host.items()}
 
     e2e = None
     if not args.no_e2e:
@@ -276,7 +279,7 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
                 "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk, "kernels": kernels}
+                "gpu_launches": launches, "clocks": clk, "kernels": kernels, "host": host_costs}
         print(json.dumps(line))
     eng.close()
     return 0

@@ -211,8 +211,10 @@ DL_API dl_status dl_run_destroy(dl_run *run);
  * admitted between any two steps (continuous batching) and leave the union
  * at their own fixpoint. Each instance's outputs, iteration count and delta
  * sizes are those of dl_run_program on the same edges and options.
- * A session owns device memory on its context's device and stream; calls on
- * one session must not run concurrently. */
+ * A session runs on its context's device and stream and takes the context's
+ * cached buffers; dl_session_destroy hands all its memory back to the
+ * context, so destroy every session before its context. Calls on one session
+ * must not run concurrently. */
 typedef struct dl_session dl_session;
 
 /* max_nodes bounds the node count of the instances alive at once (TC/SG
@@ -224,6 +226,11 @@ DL_API dl_status dl_session_create(dl_context *ctx, int32_t program, const dl_op
  * instance with no edges finishes at once. */
 DL_API dl_status dl_session_admit(dl_session *s, const int32_t *edges, int64_t rows, int32_t edges_on_device,
                                   int64_t *instance);
+/* Adds `count` instances at once (edges[i] holds rows[i] pairs); their ids
+ * are consecutive, the first one in *first_instance. One admission of many
+ * instances ranks and sorts them together. */
+DL_API dl_status dl_session_admit_many(dl_session *s, const int32_t *const *edges, const int64_t *rows,
+                                       int64_t count, int32_t edges_on_device, int64_t *first_instance);
 /* One iteration of every active instance; *active = instances still running. */
 DL_API dl_status dl_session_step(dl_session *s, int64_t *active);
 /* Ids of the instances finished since the last poll, in finishing order;

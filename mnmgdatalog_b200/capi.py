@@ -34,7 +34,7 @@ EXPORTS = (
     "dl_generate_rows", "dl_profile_enable", "dl_profile_read",
     "dl_compat_get_hash_table", "dl_compat_get_join", "dl_compat_get_join_nl",
     "dl_sort_unique_noalloc", "dl_sort_unique_noalloc_max_rows",
-    "dl_session_create", "dl_session_admit", "dl_session_step", "dl_session_poll", "dl_session_get_info",
+    "dl_session_create", "dl_session_admit", "dl_session_admit_many", "dl_session_step", "dl_session_poll", "dl_session_get_info",
     "dl_session_copy_output", "dl_session_copy_deltas", "dl_session_copy_labels", "dl_session_release",
     "dl_session_memory", "dl_session_destroy", "dl_run_batch",
 )
@@ -116,6 +116,7 @@ def lib():
         "dl_profile_read": ([vp, C.POINTER(dl_kernel_stat), i32, C.POINTER(C.c_int32)], C.c_int),
         "dl_session_create": ([vp, i32, C.POINTER(dl_options), i64, pvp], C.c_int),
         "dl_session_admit": ([vp, vp, i64, i32, pi64], C.c_int),
+        "dl_session_admit_many": ([vp, vp, vp, i64, i32, pi64], C.c_int),
         "dl_session_step": ([vp, pi64], C.c_int),
         "dl_session_poll": ([vp, vp, i64, pi64], C.c_int),
         "dl_session_get_info": ([vp, i64, C.POINTER(dl_run_info)], C.c_int),

@@ -476,6 +476,22 @@ DL_API dl_status dl_session_admit(dl_session *s, const int32_t *edges, int64_t r
     });
 }
 
+DL_API dl_status dl_session_admit_many(dl_session *s, const int32_t *const *edges, const int64_t *rows,
+                                       int64_t count, int32_t edges_on_device, int64_t *first_instance) {
+    DL_REQUIRE(s && s->s && first_instance && count >= 0 && (count == 0 || (edges && rows)), "invalid argument");
+    for (int64_t i = 0; i < count; ++i)
+        DL_REQUIRE(rows[i] >= 0 && rows[i] <= (int64_t) 0x7FFFFFFF && (edges[i] || rows[i] == 0),
+                   "invalid edge set");
+    return guarded([&] {
+        set_device(s->ctx);
+        std::vector<u64> n(count);
+        for (int64_t i = 0; i < count; ++i) n[i] = (u64) rows[i];
+        const auto ids = dl::session_admit_many(*s->s, edges, n.data(), (u64) count, edges_on_device != 0);
+        *first_instance = ids.empty() ? (int64_t) dl::session_instance_count(*s->s) : ids[0];
+        dl::session_fold_profile(*s->s, s->ctx->c);
+    });
+}
+
 DL_API dl_status dl_session_step(dl_session *s, int64_t *active) {
     DL_REQUIRE(s && s->s, "invalid argument");
     return guarded([&] {
@@ -568,7 +584,9 @@ DL_API dl_status dl_run_batch(dl_context *ctx, int32_t program, const int32_t *c
     if (st != DL_OK) return st;
     st = guarded([&] {
         set_device(ctx);
-        for (int64_t i = 0; i < count; ++i) dl::session_admit(*s->s, edges[i], (u64) rows[i], edges_on_device != 0);
+        std::vector<u64> n(count);
+        for (int64_t i = 0; i < count; ++i) n[i] = (u64) rows[i];
+        dl::session_admit_many(*s->s, edges, n.data(), (u64) count, edges_on_device != 0);
         while (dl::session_step(*s->s) > 0) {
         }
         dl::session_fold_profile(*s->s, ctx->c);

@@ -1,7 +1,15 @@
 // Context: device, stream, control block, grow-only scratch.
+#include <chrono>
+
 #include "dl_internal.h"
 
 namespace dl {
+
+namespace {
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
 
 void DevBuf::reserve(size_t bytes, bool zero) {
     if (bytes <= cap && p) return;
@@ -27,13 +35,22 @@ void DevBuf::release() {
 
 void Context::reserve(DevBuf &buf, size_t bytes, bool zero) {
     if (buf.p && buf.cap >= bytes) return;
+    // A buffer that outgrows itself grows by half at least, so a relation that
+    // grows every iteration is reallocated O(log) times, not at every step.
+    const size_t want = buf.p ? std::max(bytes, buf.cap + buf.cap / 2) : bytes;
+    // Best fit among the cached buffers, but never one far larger than the
+    // request: a small result must not pin a large buffer that a growing
+    // relation will need next.
+    const size_t limit = std::max<size_t>(4 * bytes, bytes + (size_t(64) << 20));
     int best = -1;
     for (int i = 0; i < (int) spares.size(); ++i)
-        if (spares[i].cap >= bytes && (best < 0 || spares[i].cap < spares[best].cap)) best = i;
+        if (spares[i].cap >= bytes && spares[i].cap <= limit && (best < 0 || spares[i].cap < spares[best].cap))
+            best = i;
     if (best >= 0) {
-        buf.release();
+        if (buf.p) spares.push_back(buf);
         buf = spares[best];
         spares.erase(spares.begin() + best);
+        trim_spares();
         if (zero) DL_CUDA(cudaMemsetAsync(buf.p, 0, buf.cap, stream));
         return;
     }
@@ -41,14 +58,45 @@ void Context::reserve(DevBuf &buf, size_t bytes, bool zero) {
         // Keep the old allocation for smaller requests later.
         spares.push_back(buf);
         buf = DevBuf();
+        trim_spares();
     }
+    allocate(buf, want, zero, bytes);
+}
+
+void Context::allocate(DevBuf &buf, size_t bytes, bool zero, size_t minimum) {
+    const double t0 = now_s();
     try {
         buf.reserve(bytes, zero);
     } catch (const Error &) {
-        // Out of memory: drop every spare and retry once.
+        // Out of memory: drop every cached buffer and retry once.
         for (auto &s : spares) s.release();
         spares.clear();
-        buf.reserve(bytes, zero);
+        buf.reserve(minimum ? minimum : bytes, zero);
+    }
+    KernelStat &k = kstat[K_HOST_MALLOC];
+    k.launches++;
+    k.timed++;
+    k.seconds += now_s() - t0;
+    k.bytes += (double) buf.cap;
+}
+
+void Context::trim_spares() {
+    // Cache at most kSpareCount buffers and kSpareBytes in total, freeing the
+    // smallest first (large buffers are the expensive ones to re-create).
+    size_t total = 0;
+    for (const auto &s : spares) total += s.cap;
+    while (spares.size() > kSpareCount || total > kSpareBytes) {
+        int small = 0;
+        for (int i = 1; i < (int) spares.size(); ++i)
+            if (spares[i].cap < spares[small].cap) small = i;
+        total -= spares[small].cap;
+        const double t0 = now_s();
+        kstat[K_HOST_FREE].bytes += (double) spares[small].cap;
+        spares[small].release();
+        kstat[K_HOST_FREE].seconds += now_s() - t0;
+        kstat[K_HOST_FREE].launches++;
+        kstat[K_HOST_FREE].timed++;
+        spares.erase(spares.begin() + small);
     }
 }
 
@@ -56,14 +104,7 @@ void Context::give_back(DevBuf &buf) {
     if (!buf.p) return;
     spares.push_back(buf);
     buf = DevBuf();
-    while (spares.size() > 6) {
-        // Free the smallest spare.
-        int small = 0;
-        for (int i = 1; i < (int) spares.size(); ++i)
-            if (spares[i].cap < spares[small].cap) small = i;
-        spares[small].release();
-        spares.erase(spares.begin() + small);
-    }
+    trim_spares();
 }
 
 void Context::release_all() {
@@ -75,7 +116,7 @@ void Context::release_all() {
     DevBuf *all[] = {&ws.input, &ws.ids, &ws.w0, &ws.w1, &ws.csr_off, &ws.csr_val, &ws.full[0], &ws.full[1],
                      &ws.small[0], &ws.small[1], &ws.sample,
                      &ws.jbuf[0], &ws.jbuf[1], &ws.offsets, &ws.wcc_label, &ws.wcc_flag, &ws.wcc_next,
-                     &lookback, &sort_hist, &lbs_splits, &radix_part};
+                     &lookback, &sort_hist, &lbs_splits, &radix_part, &merge_splits};
     for (DevBuf *b : all) b->release();
 }
 
@@ -114,7 +155,7 @@ const char *kernel_name(int kid) {
     static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_spine_scan", "sort_scatter_pass",
                                          "select_compact", "join_count_scan", "join_partition", "join_emit",
                                          "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build",
-                                         "sparse_diff"};
+                                         "sparse_diff", "host_cudaMalloc", "host_cudaFree", "host_sync"};
     return (kid >= 0 && kid < K_COUNT) ? names[kid] : "?";
 }
 
@@ -172,7 +213,12 @@ void Context::prof_reset() {
 void Context::sync() {
     DL_CUDA(cudaMemcpyAsync(reinterpret_cast<u32 *>(host_scalars) + 2 * 63, &ctrl->err, sizeof(u32),
                             cudaMemcpyDeviceToHost, stream));
+    const double t0 = now_s();
     DL_CUDA(cudaStreamSynchronize(stream));
+    KernelStat &k = kstat[K_HOST_SYNC];
+    k.launches++;
+    k.timed++;
+    k.seconds += now_s() - t0;
     if (!pending.empty()) prof_resolve();
     check_device_error();
 }

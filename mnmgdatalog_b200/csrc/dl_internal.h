@@ -74,6 +74,10 @@ enum KernelId : int {
     K_MERGE,           // plain merge: 16 B per word
     K_HASH_BUILD,      // C-ABI hash table insert / value extraction
     K_SPARSE_DIFF,     // sparse set difference probes (+ run sampling)
+    // host-side costs, counted with or without profiling (seconds = host wall time)
+    K_HOST_MALLOC,     // cudaMalloc of a buffer that had to grow (bytes = size)
+    K_HOST_FREE,       // cudaFree of a cached buffer dropped from the cache
+    K_HOST_SYNC,       // host waits for the stream (cudaStreamSynchronize)
     K_COUNT
 };
 const char *kernel_name(int kid);
@@ -110,10 +114,16 @@ struct Context {
     DevBuf sort_hist;               // radix histograms / bucket bases
     DevBuf lbs_splits;              // join emit partition points
     DevBuf radix_part;              // per-(digit, CTA) counts and offsets of a radix pass
+    DevBuf merge_splits;            // merge-path split points of a set operation
     u64 *host_scalars = nullptr;    // pinned mirror for small D2H reads
     Workspace ws;
     u64 run_join_total = 0, run_join_max = 0;  // join statistics of the current run
-    std::vector<DevBuf> spares;     // buffers handed back by destroyed runs
+    std::vector<DevBuf> spares;     // buffers handed back by destroyed runs and sessions
+    // Freeing a multi-GB buffer costs milliseconds and synchronises the
+    // device, so outgrown buffers stay cached; an allocation that fails
+    // drops the whole cache and retries (Context::allocate).
+    static constexpr size_t kSpareCount = 256;
+    static constexpr size_t kSpareBytes = 96ull << 30;
 
     // Live profile: every launch is counted; with prof_on each launch is
     // bracketed by events that are resolved at the next sync().
@@ -136,6 +146,10 @@ struct Context {
     // Ensure buf holds `bytes`, preferring a spare buffer over cudaMalloc.
     void reserve(DevBuf &buf, size_t bytes, bool zero = false);
     void give_back(DevBuf &buf);
+    void trim_spares();
+    // Fresh allocation of `bytes` into an empty buf; on failure frees every
+    // cached buffer and tries once more (with `minimum` bytes if given).
+    void allocate(DevBuf &buf, size_t bytes, bool zero = false, size_t minimum = 0);
     void release_all();
 
     // Next look-back epoch; clears the look-back buffer when the 14-bit epoch

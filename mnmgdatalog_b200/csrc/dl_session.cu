@@ -31,33 +31,70 @@ using namespace detail;
 #define GRID_STRIDE(i, n) \
     for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (u64) gridDim.x * blockDim.x)
 
-// Rows (a, b) of one instance -> fwd (rank a, rank b) / rev (rank b, rank a)
-// words over union ranks (instance ranks start at `base`).
-__global__ void session_pack_kernel(const int32_t *__restrict__ rows, u64 n, const int32_t *__restrict__ ids, u32 n_ids,
-                                    u64 base, int bits, u64 *__restrict__ fwd, u64 *__restrict__ rev) {
-    GRID_STRIDE(i, n) {
-        const int32_t a = rows[2 * i], b = rows[2 * i + 1];
-        u32 lo = 0, hi = n_ids;
-        while (lo < hi) {
-            const u32 m = (lo + hi) >> 1;
-            if (ids[m] < a) lo = m + 1;
-            else hi = m;
-        }
-        const u64 ra = base + lo;
-        lo = 0;
-        hi = n_ids;
-        while (lo < hi) {
-            const u32 m = (lo + hi) >> 1;
-            if (ids[m] < b) lo = m + 1;
-            else hi = m;
-        }
-        const u64 rb = base + lo;
-        if (fwd) fwd[i] = (ra << bits) | rb;
-        if (rev) rev[i] = (rb << bits) | ra;
+// Instance of row r of a concatenation: last k with off[k] <= r.
+__device__ __forceinline__ u32 segment_of(const u64 *__restrict__ off, u32 count, u64 r) {
+    u32 a = 0, b = count;
+    while (a < b) {
+        const u32 m = (a + b) >> 1;
+        if (off[m] <= r) a = m + 1;
+        else b = m;
+    }
+    return a - 1;
+}
+
+// (instance << 32 | biased node id) for both columns of every row.
+__global__ void session_tag_kernel(const int32_t *__restrict__ rows, u64 n, const u64 *__restrict__ off, u32 count,
+                                   u64 *__restrict__ out) {
+    GRID_STRIDE(r, n) {
+        const u64 k = (u64) segment_of(off, count, r) << 32;
+        out[2 * r] = k | ((u32) rows[2 * r] ^ 0x80000000u);
+        out[2 * r + 1] = k | ((u32) rows[2 * r + 1] ^ 0x80000000u);
     }
 }
 
-// Appends one instance's sorted words to the union offset table:
+// first[k] = index of the first tagged word of instance k (k in [0, count]).
+__global__ void session_first_kernel(const u64 *__restrict__ u, u64 nu, u32 count, u64 *__restrict__ first) {
+    GRID_STRIDE(k, (u64) count + 1) {
+        const u64 target = k << 32;
+        u64 l = 0, h = nu;
+        while (l < h) {
+            const u64 m = (l + h) >> 1;
+            if (u[m] < target) l = m + 1;
+            else h = m;
+        }
+        first[k] = l;
+    }
+}
+
+__global__ void session_ids_kernel(const u64 *__restrict__ u, u64 nu, int32_t *__restrict__ ids) {
+    GRID_STRIDE(i, nu) ids[i] = (int32_t) ((u32) u[i] ^ 0x80000000u);
+}
+
+__device__ __forceinline__ u64 lower_bound_u64(const u64 *__restrict__ a, u64 n, u64 x) {
+    u64 l = 0, h = n;
+    while (l < h) {
+        const u64 m = (l + h) >> 1;
+        if (a[m] < x) l = m + 1;
+        else h = m;
+    }
+    return l;
+}
+
+// Rows of many instances -> words over union ranks (rank = base + position
+// of (instance, id) among the sorted distinct tagged ids).
+__global__ void session_pack_many_kernel(const int32_t *__restrict__ rows, u64 n, const u64 *__restrict__ off,
+                                         u32 count, const u64 *__restrict__ u, u64 nu, u64 base, int bits,
+                                         u64 *__restrict__ fwd, u64 *__restrict__ rev) {
+    GRID_STRIDE(r, n) {
+        const u64 k = (u64) segment_of(off, count, r) << 32;
+        const u64 ra = base + lower_bound_u64(u, nu, k | ((u32) rows[2 * r] ^ 0x80000000u));
+        const u64 rb = base + lower_bound_u64(u, nu, k | ((u32) rows[2 * r + 1] ^ 0x80000000u));
+        if (fwd) fwd[r] = (ra << bits) | rb;
+        if (rev) rev[r] = (rb << bits) | ra;
+    }
+}
+
+// Appends the sorted words of ranks [lo, hi) to the union offset table:
 // off[r] = base + (first word with key >= r) for r in [lo, hi].
 __global__ void session_csr_kernel(const u64 *__restrict__ w, u64 n, int bits, u64 lo, u64 hi, u64 base,
                                    u32 *__restrict__ off, u32 *__restrict__ val) {
@@ -106,17 +143,15 @@ __global__ void session_hist_kernel(const u64 *__restrict__ d, u64 n, int shift,
             if (sh[i]) atomicAdd(&cnt[i], (unsigned long long) sh[i]);
 }
 
-// [first, end) of the words with key rank in [rlo, rhi) of a sorted run.
-__global__ void session_bounds_kernel(const u64 *__restrict__ w, u64 n, u64 klo, u64 khi, u64 *__restrict__ out) {
-    if (threadIdx.x < 2) {
-        const u64 target = threadIdx.x == 0 ? klo : khi;
-        u64 l = 0, h = n;
-        while (l < h) {
-            const u64 m = (l + h) >> 1;
-            if (w[m] < target) l = m + 1;
-            else h = m;
-        }
-        out[threadIdx.x] = l;
+// Word ranges of instances in the two sorted runs: for instance k (ranks
+// lohi[k] .. lohi[n + k]) out[4k..4k+3] = [first, end) in `big`, then in `small`.
+__global__ void session_bounds_kernel(const u64 *__restrict__ big, u64 nbig, const u64 *__restrict__ small,
+                                      u64 nsmall, const u64 *__restrict__ lohi, u32 n, int bits,
+                                      u64 *__restrict__ out) {
+    GRID_STRIDE(t, 4 * (u64) n) {
+        const u64 k = t >> 2, which = t & 3;
+        const u64 target = (which & 1 ? lohi[n + k] : lohi[k]) << bits;
+        out[t] = which < 2 ? lower_bound_u64(big, nbig, target) : lower_bound_u64(small, nsmall, target);
     }
 }
 
@@ -139,9 +174,18 @@ __global__ void session_next_delta_kernel(const u32 *__restrict__ nodes, u64 cou
     }
 }
 
-// Components of one instance: counts of the labels of ranks [lo, hi).
-__global__ void session_wcc_count_kernel(const u32 *__restrict__ label, u64 lo, u64 hi, u32 *__restrict__ cnt) {
-    GRID_STRIDE(i, hi - lo) atomicAdd(&cnt[label[lo + i] - lo], 1u);
+// Slot t of a concatenation of instance rank ranges (instance k from slot
+// off[k], ranks lo[k]...): counts the component label of the node into
+// cnt[off[k] + label - lo[k]] and copies the node's label.
+__global__ void session_wcc_count_kernel(const u32 *__restrict__ label, const u64 *__restrict__ lo,
+                                         const u64 *__restrict__ off, u32 n, u64 total, u32 *__restrict__ cnt,
+                                         u32 *__restrict__ labels_out) {
+    GRID_STRIDE(t, total) {
+        const u32 k = segment_of(off, n, t);
+        const u32 l = label[lo[k] + (t - off[k])];
+        labels_out[t] = l;
+        atomicAdd(&cnt[off[k] + (l - lo[k])], 1u);
+    }
 }
 
 struct NonZero {
@@ -149,13 +193,18 @@ struct NonZero {
     __device__ __forceinline__ u64 degree(u64 i) const { return c[i] != 0u; }
 };
 
-__global__ void session_wcc_comp_kernel(const u32 *__restrict__ cnt, u64 n, const u64 *__restrict__ pos,
-                                        u32 *__restrict__ comp, unsigned long long *__restrict__ largest) {
-    GRID_STRIDE(c, n) {
-        const u32 k = cnt[c];
-        if (k) {
-            comp[pos[c]] = (u32) c;
-            atomicMax(largest, (unsigned long long) k);
+// Components of every instance (local ranks, ascending), the largest size
+// per instance, and where each instance's components start.
+__global__ void session_wcc_comp_kernel(const u32 *__restrict__ cnt, const u64 *__restrict__ pos,
+                                        const u64 *__restrict__ off, u32 n, u64 total, u32 *__restrict__ comp,
+                                        unsigned long long *__restrict__ largest, u64 *__restrict__ start) {
+    GRID_STRIDE(t, total) {
+        const u32 k = segment_of(off, n, t);
+        if (t == off[k]) start[k] = pos[t];
+        const u32 c = cnt[t];
+        if (c) {
+            comp[pos[t]] = (u32) (t - off[k]);
+            atomicMax(&largest[k], (unsigned long long) c);
         }
     }
 }
@@ -223,7 +272,7 @@ u64 session_select(Context &ctx, u64 *buf, u64 n, Keep keep, int slot) {
 void grow_keep(Context &ctx, DevBuf &b, size_t bytes, size_t keep) {
     if (b.p && b.cap >= bytes) return;
     DevBuf nb;
-    nb.reserve(std::max(bytes, b.cap * 3 / 2));
+    ctx.allocate(nb, std::max(bytes, b.cap * 3 / 2));
     if (keep && b.p) DL_CUDA(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice, ctx.stream));
     ctx.sync();
     b.release();
@@ -234,6 +283,7 @@ void grow_keep(Context &ctx, DevBuf &b, size_t bytes, size_t keep) {
 
 struct SessionImpl {
     Context ctx;  // private workspace; shares the caller's stream
+    Context *parent = nullptr;
     int program = DL_PROGRAM_TC;
     dl_options opt{};
     int bits = 30;
@@ -247,7 +297,9 @@ struct SessionImpl {
     u64 n_delta = 0;
     DevBuf label, flag, nextl;  // WCC
     DevBuf inst_lo, inst_hi;    // device copies of the active instances' rank ranges
-    DevBuf counts;              // per active instance delta counts
+    DevBuf counts;              // per instance delta counts
+    DevBuf range_lo;            // first ranks of the instances of a range count
+    DevBuf admit_off, admit_first;  // row offsets / first tagged ids of an admission
     DevBuf live;                // per active instance flag (WCC freezing)
     std::vector<SessionInstance> inst;
     std::vector<i64> active;    // instance ids in rank order
@@ -312,71 +364,144 @@ void upload_active(SessionImpl &s) {
     s.inst_dirty = false;
 }
 
-// Per-active-instance counts of the words in d (rank = word >> shift).
-std::vector<u64> delta_counts(SessionImpl &s, const u64 *d, u64 n, int shift) {
+// Counts of the words of d (rank = word >> shift) per instance, given the
+// instances' first ranks in increasing order on the device.
+std::vector<u64> counts_by_lo(SessionImpl &s, const u64 *d, u64 n, int shift, const u64 *d_lo, u64 na) {
     Context &ctx = s.ctx;
-    const u64 na = s.active.size();
     std::vector<u64> c(na, 0);
-    if (na == 0) return c;
-    if (n == 0) return c;
-    upload_active(s);
+    if (na == 0 || n == 0) return c;
     ctx.reserve(s.counts, na * 8);
     DL_CUDA(cudaMemsetAsync(s.counts.p, 0, na * 8, ctx.stream));
     const unsigned smem = na <= 8192 ? (unsigned) (na * 4) : 0u;
     DL_LAUNCH(ctx, K_PREP, 8.0 * n,
               session_hist_kernel<<<grid_for(n, 256, ctx, 8), 256, smem, ctx.stream>>>(
-                  d, n, shift, s.inst_lo.as<u64>(), (u32) na, (unsigned long long *) s.counts.p));
+                  d, n, shift, d_lo, (u32) na, (unsigned long long *) s.counts.p));
     DL_CUDA(cudaMemcpyAsync(c.data(), s.counts.p, na * 8, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
     return c;
 }
 
-// Sorted words of one TC/SG instance out of both full runs.
-void extract_words(SessionImpl &s, SessionInstance &in) {
-    Context &ctx = s.ctx;
-    Workspace &ws = ctx.ws;
-    const u64 klo = in.rank_lo << s.bits, khi = in.rank_hi << s.bits;
-    u64 *bnd = &ctx.ctrl->scalar[20];
-    DL_LAUNCH(ctx, K_PREP, 0,
-              session_bounds_kernel<<<1, 32, 0, ctx.stream>>>(ws.full[s.F.cur].as<u64>(), s.F.nbig, klo, khi, bnd));
-    DL_LAUNCH(ctx, K_PREP, 0,
-              session_bounds_kernel<<<1, 32, 0, ctx.stream>>>(ws.small[s.F.scur].as<u64>(), s.F.nsmall, klo, khi,
-                                                               bnd + 2));
-    DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 8, bnd, 32, cudaMemcpyDeviceToHost, ctx.stream));
-    ctx.sync();
-    const u64 *hb = ctx.host_scalars + 8;
-    const u64 a0 = hb[0], na = hb[1] - hb[0], b0 = hb[2], nb = hb[3] - hb[2];
-    in.n_result = na + nb;
-    ctx.reserve(in.result, std::max<u64>(in.n_result, 1) * 8);
-    if (in.n_result)
-        merge_words(ctx, ws.full[s.F.cur].as<u64>() + a0, na, ws.small[s.F.scur].as<u64>() + b0, nb,
-                    in.result.as<u64>(), Codec::Raw);
-    s.dead += in.n_result;
+// Per-active-instance counts.
+std::vector<u64> delta_counts(SessionImpl &s, const u64 *d, u64 n, int shift) {
+    if (s.active.empty() || n == 0) return std::vector<u64>(s.active.size(), 0);
+    upload_active(s);
+    return counts_by_lo(s, d, n, shift, s.inst_lo.as<u64>(), s.active.size());
 }
 
-void extract_components(SessionImpl &s, SessionInstance &in) {
+// Counts for the instances whose first ranks are `lo` (increasing).
+std::vector<u64> range_counts(SessionImpl &s, const u64 *d, u64 n, int shift, const std::vector<u64> &lo) {
+    if (lo.empty() || n == 0) return std::vector<u64>(lo.size(), 0);
+    s.ctx.reserve(s.range_lo, lo.size() * 8);
+    DL_CUDA(cudaMemcpyAsync(s.range_lo.p, lo.data(), lo.size() * 8, cudaMemcpyHostToDevice, s.ctx.stream));
+    return counts_by_lo(s, d, n, shift, s.range_lo.as<u64>(), lo.size());  // syncs before `lo` goes
+}
+
+// A device block shared by the instances extracted or admitted together; its
+// memory returns to the session's buffer cache with the last instance.
+std::shared_ptr<DevBuf> make_block(Context &ctx, size_t bytes) {
+    DevBuf *b = new DevBuf;
+    try {
+        ctx.reserve(*b, std::max<size_t>(bytes, 8));
+    } catch (...) {
+        delete b;
+        throw;
+    }
+    Context *c = &ctx;
+    return std::shared_ptr<DevBuf>(b, [c](DevBuf *x) {
+        c->give_back(*x);
+        delete x;
+    });
+}
+
+// Uploads the rank ranges of `ids` ([lo..., hi...]) to s.range_lo.
+void upload_ranges(SessionImpl &s, const std::vector<i64> &ids) {
+    const u64 n = ids.size();
+    std::vector<u64> h(2 * n);
+    for (u64 k = 0; k < n; ++k) {
+        h[k] = s.inst[ids[k]].rank_lo;
+        h[n + k] = s.inst[ids[k]].rank_hi;
+    }
+    s.ctx.reserve(s.range_lo, 2 * n * 8);
+    DL_CUDA(cudaMemcpyAsync(s.range_lo.p, h.data(), 2 * n * 8, cudaMemcpyHostToDevice, s.ctx.stream));
+    s.ctx.sync();  // h is a host temporary
+}
+
+// Sorted words of finished TC/SG instances out of both full runs, into one
+// block (each instance's words are a key range of each run).
+void extract_words(SessionImpl &s, const std::vector<i64> &ids) {
     Context &ctx = s.ctx;
-    const u64 n = in.rank_hi - in.rank_lo;
-    DevBuf cnt, pos;
-    ctx.reserve(cnt, std::max<u64>(n, 1) * 4);
-    ctx.reserve(pos, std::max<u64>(n, 1) * 8);
-    DL_CUDA(cudaMemsetAsync(cnt.p, 0, n * 4, ctx.stream));
+    Workspace &ws = ctx.ws;
+    const u64 n = ids.size();
+    upload_ranges(s, ids);
+    ctx.reserve(s.counts, 4 * n * 8);
+    const u64 *big = ws.full[s.F.cur].as<u64>(), *small = ws.small[s.F.scur].as<u64>();
     DL_LAUNCH(ctx, K_PREP, 0,
-              session_wcc_count_kernel<<<grid_for(n, 256, ctx, 8), 256, 0, ctx.stream>>>(s.label.as<u32>(), in.rank_lo,
-                                                                                         in.rank_hi, cnt.as<u32>()));
-    const u64 nc = count_matches(ctx, NonZero{cnt.as<u32>()}, n, pos.as<u64>());
-    u64 *largest = &ctx.ctrl->scalar[24];
-    DL_CUDA(cudaMemsetAsync(largest, 0, 8, ctx.stream));
-    ctx.reserve(in.result, std::max<u64>(nc, 1) * 4);
-    DL_LAUNCH(ctx, K_PREP, 0,
-              session_wcc_comp_kernel<<<grid_for(n, 256, ctx, 8), 256, 0, ctx.stream>>>(
-                  cnt.as<u32>(), n, pos.as<u64>(), in.result.as<u32>(), (unsigned long long *) largest));
-    ctx.reserve(in.labels, std::max<u64>(n, 1) * 4);
-    DL_CUDA(cudaMemcpyAsync(in.labels.p, s.label.as<u32>() + in.rank_lo, n * 4, cudaMemcpyDeviceToDevice, ctx.stream));
-    DL_CUDA(cudaMemcpyAsync(ctx.host_scalars + 12, largest, 8, cudaMemcpyDeviceToHost, ctx.stream));
+              session_bounds_kernel<<<grid_for(4 * n, 256, ctx, 4), 256, 0, ctx.stream>>>(
+                  big, s.F.nbig, small, s.F.nsmall, s.range_lo.as<u64>(), (u32) n, s.bits, s.counts.as<u64>()));
+    std::vector<u64> hb(4 * n);
+    DL_CUDA(cudaMemcpyAsync(hb.data(), s.counts.p, 4 * n * 8, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
-    in.n_result = nc;
-    in.largest = (i64) ctx.host_scalars[12];
+    u64 total = 0;
+    for (u64 k = 0; k < n; ++k) total += (hb[4 * k + 1] - hb[4 * k]) + (hb[4 * k + 3] - hb[4 * k + 2]);
+    auto block = make_block(ctx, total * 8);
+    u64 at = 0;
+    for (u64 k = 0; k < n; ++k) {
+        SessionInstance &in = s.inst[ids[k]];
+        const u64 a0 = hb[4 * k], na = hb[4 * k + 1] - a0, b0 = hb[4 * k + 2], nb = hb[4 * k + 3] - b0;
+        u64 *dst = block->as<u64>() + at;
+        if (na && nb) merge_words(ctx, big + a0, na, small + b0, nb, dst, Codec::Raw);
+        else if (na) DL_CUDA(cudaMemcpyAsync(dst, big + a0, na * 8, cudaMemcpyDeviceToDevice, ctx.stream));
+        else if (nb) DL_CUDA(cudaMemcpyAsync(dst, small + b0, nb * 8, cudaMemcpyDeviceToDevice, ctx.stream));
+        in.result_block = block;
+        in.result_off = at;
+        in.n_result = na + nb;
+        at += na + nb;
+        s.dead += na + nb;
+    }
+}
+
+// Components (ascending local ranks), largest component and per-node labels
+// of finished WCC instances, all in one pass over their rank ranges.
+void extract_components(SessionImpl &s, const std::vector<i64> &ids) {
+    Context &ctx = s.ctx;
+    const u64 n = ids.size();
+    std::vector<u64> off(n + 1, 0);
+    for (u64 k = 0; k < n; ++k) off[k + 1] = off[k] + s.inst[ids[k]].n_ids;
+    const u64 total = off[n];
+    upload_ranges(s, ids);
+    // s.counts: slot offsets [n + 1] then largest [n] then component starts [n]
+    ctx.reserve(s.counts, (3 * n + 1) * 8);
+    u64 *d_off = s.counts.as<u64>(), *d_big = d_off + n + 1, *d_start = d_big + n;
+    DL_CUDA(cudaMemcpyAsync(d_off, off.data(), (n + 1) * 8, cudaMemcpyHostToDevice, ctx.stream));
+    DL_CUDA(cudaMemsetAsync(d_big, 0, n * 8, ctx.stream));
+    DevBuf cnt, pos;
+    ctx.reserve(cnt, std::max<u64>(total, 1) * 4);
+    ctx.reserve(pos, std::max<u64>(total, 1) * 8);
+    DL_CUDA(cudaMemsetAsync(cnt.p, 0, total * 4, ctx.stream));
+    auto labels = make_block(ctx, total * 4);
+    const u64 *lo = s.range_lo.as<u64>();
+    DL_LAUNCH(ctx, K_PREP, 0,
+              session_wcc_count_kernel<<<grid_for(total, 256, ctx, 8), 256, 0, ctx.stream>>>(
+                  s.label.as<u32>(), lo, d_off, (u32) n, total, cnt.as<u32>(), labels->as<u32>()));
+    const u64 nc = count_matches(ctx, NonZero{cnt.as<u32>()}, total, pos.as<u64>());
+    auto comps = make_block(ctx, nc * 4);
+    DL_LAUNCH(ctx, K_PREP, 0,
+              session_wcc_comp_kernel<<<grid_for(total, 256, ctx, 8), 256, 0, ctx.stream>>>(
+                  cnt.as<u32>(), pos.as<u64>(), d_off, (u32) n, total, comps->as<u32>(),
+                  (unsigned long long *) d_big, d_start));
+    std::vector<u64> h(2 * n);
+    DL_CUDA(cudaMemcpyAsync(h.data(), d_big, 2 * n * 8, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    for (u64 k = 0; k < n; ++k) {
+        SessionInstance &in = s.inst[ids[k]];
+        const u64 start = h[n + k], end = k + 1 < n ? h[n + k + 1] : nc;
+        in.result_block = comps;
+        in.result_off = start;
+        in.n_result = end - start;
+        in.largest = (i64) h[k];
+        in.labels_block = labels;
+        in.labels_off = off[k];
+    }
     ctx.give_back(cnt);
     ctx.give_back(pos);
 }
@@ -387,11 +512,11 @@ void mark_done(SessionImpl &s, SessionInstance &in) {
     s.finished.push_back(in.id);
 }
 
-void finish(SessionImpl &s, i64 id) {
-    SessionInstance &in = s.inst[id];
-    if (s.program == DL_PROGRAM_WCC) extract_components(s, in);
-    else extract_words(s, in);
-    mark_done(s, in);
+void finish(SessionImpl &s, const std::vector<i64> &ids) {
+    if (ids.empty()) return;
+    if (s.program == DL_PROGRAM_WCC) extract_components(s, ids);
+    else extract_words(s, ids);
+    for (i64 id : ids) mark_done(s, s.inst[id]);
 }
 
 // Drops the union state once no instance is active: ranks, offsets and the
@@ -435,7 +560,7 @@ void maybe_compact(SessionImpl &s) {
 }
 
 void retire(SessionImpl &s, const std::vector<i64> &done, const std::vector<i64> &still) {
-    for (i64 id : done) finish(s, id);
+    finish(s, done);
     if (still.size() != s.active.size()) {
         s.active = still;
         s.inst_dirty = true;
@@ -563,6 +688,7 @@ SessionImpl *session_create(Context &parent, int program, const dl_options &opt,
         s->rank_cap = 1ull << s->bits;
     }
     Context &c = s->ctx;
+    s->parent = &parent;
     c.device = parent.device;
     c.stream = parent.stream;
     c.sm_count = parent.sm_count;
@@ -573,6 +699,8 @@ SessionImpl *session_create(Context &parent, int program, const dl_options &opt,
     DL_CUDA(cudaMemset(p, 0, sizeof(Ctrl)));
     DL_CUDA(cudaMallocHost((void **) &c.host_scalars, 64 * sizeof(u64)));
     std::memset(c.host_scalars, 0, 64 * sizeof(u64));
+    c.spares = std::move(parent.spares);  // the parent's cached buffers serve the session
+    parent.spares.clear();
     return s.release();
 }
 
@@ -580,74 +708,128 @@ void session_destroy(SessionImpl *s) {
     if (!s) return;
     Context &c = s->ctx;
     cudaStreamSynchronize(c.stream);
-    for (auto &in : s->inst) {
-        in.ids.release();
-        in.result.release();
-        in.labels.release();
+    c.prof_resolve();
+    // Every buffer goes back to the parent context's cache: the next run or
+    // session on it reuses the memory instead of allocating it again.
+    Context &p = *s->parent;
+    for (auto &in : s->inst) {  // blocks return to the session's cache
+        in.ids_block.reset();
+        in.result_block.reset();
+        in.labels_block.reset();
     }
-    DevBuf *bufs[] = {&s->off,  &s->val,     &s->delta,   &s->label,  &s->flag,
-                      &s->nextl, &s->inst_lo, &s->inst_hi, &s->counts, &s->live};
-    for (DevBuf *b : bufs) b->release();
-    c.release_all();
+    DevBuf *bufs[] = {&s->off,     &s->val,    &s->delta,    &s->label,     &s->flag,
+                      &s->nextl,   &s->inst_lo, &s->inst_hi, &s->counts,    &s->live,
+                      &s->range_lo, &s->admit_off, &s->admit_first};
+    for (DevBuf *b : bufs) p.give_back(*b);
+    Workspace &w = c.ws;
+    DevBuf *wbufs[] = {&w.input,    &w.ids,      &w.w0,       &w.w1,      &w.csr_off,  &w.csr_val,
+                       &w.full[0],  &w.full[1],  &w.small[0], &w.small[1], &w.sample,  &w.jbuf[0],
+                       &w.jbuf[1],  &w.offsets,  &w.wcc_label, &w.wcc_flag, &w.wcc_next};
+    for (DevBuf *b : wbufs) p.give_back(*b);
+    for (auto &b : c.spares) p.give_back(b);
+    c.spares.clear();
+    c.release_all();  // look-back words, histograms, split points, events
     if (c.ctrl) cudaFree(c.ctrl);
     if (c.host_scalars) cudaFreeHost(c.host_scalars);
     delete s;
 }
 
-i64 session_admit(SessionImpl &s, const int32_t *rows_in, u64 n, bool on_device) {
+std::vector<i64> session_admit_many(SessionImpl &s, const int32_t *const *rows, const u64 *nrows, u64 count,
+                                    bool on_device) {
     Context &ctx = s.ctx;
     Workspace &ws = ctx.ws;
-    s.inst.emplace_back();
-    SessionInstance &in = s.inst.back();
-    in.id = (i64) s.inst.size() - 1;
-    in.input_rows = (i64) n;
-    in.rank_lo = in.rank_hi = s.next_rank;
-    if (n == 0) {  // the program never enters its loop: zero iterations, empty result
-        mark_done(s, in);
-        return in.id;
+    if (count >= (1ull << 31)) throw Error(DL_ERR_INVALID_ARGUMENT, "too many instances in one admission");
+    std::vector<u64> off(count + 1, 0);
+    for (u64 k = 0; k < count; ++k) off[k + 1] = off[k] + nrows[k];
+    const u64 N = off[count];
+    const u64 first_id = s.inst.size();
+    std::vector<i64> ids(count);
+    for (u64 k = 0; k < count; ++k) {
+        s.inst.emplace_back();
+        SessionInstance &in = s.inst.back();
+        in.id = (i64) (first_id + k);
+        in.input_rows = (i64) nrows[k];
+        in.rank_lo = in.rank_hi = s.next_rank;
+        ids[k] = in.id;
+    }
+    auto inst = [&](u64 k) -> SessionInstance & { return s.inst[first_id + k]; };
+    if (N == 0) {  // no instance enters its loop: zero iterations, empty results
+        for (u64 k = 0; k < count; ++k) mark_done(s, inst(k));
+        return ids;
     }
     try {
-        const int32_t *rows = stage_input(ctx, rows_in, n, on_device);
-        Graph gi;
-        rank_nodes(ctx, rows, n, gi);  // distinct ids of this instance, sorted, in ws.ids
-        const u64 nid = gi.n_ids;
-        if (s.next_rank + nid > s.rank_cap)
-            throw Error(DL_ERR_OVERFLOW, "session node capacity exhausted (" + std::to_string(s.rank_cap) + " ranks)");
-        ctx.reserve(in.ids, nid * 4);
-        DL_CUDA(cudaMemcpyAsync(in.ids.p, gi.ids, nid * 4, cudaMemcpyDeviceToDevice, ctx.stream));
-        in.n_ids = (u32) nid;
-        in.rank_lo = s.next_rank;
-        in.rank_hi = s.next_rank + nid;
-        const bool wcc = s.program == DL_PROGRAM_WCC;
-        const u64 m = wcc ? 2 * n : n;
+        // every instance's rows, back to back, and their row offsets
+        ctx.reserve(ws.input, N * 8);
+        for (u64 k = 0; k < count; ++k)
+            if (nrows[k])
+                DL_CUDA(cudaMemcpyAsync(ws.input.as<int32_t>() + 2 * off[k], rows[k], nrows[k] * 8,
+                                        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx.stream));
+        ctx.reserve(s.admit_off, (count + 1) * 8);
+        DL_CUDA(cudaMemcpyAsync(s.admit_off.p, off.data(), (count + 1) * 8, cudaMemcpyHostToDevice, ctx.stream));
+        const int32_t *in_rows = ws.input.as<int32_t>();
+        const u64 *d_off = s.admit_off.as<u64>();
+        // distinct (instance, node id) pairs, sorted: position = union rank
+        // offset (tc.cu:171-176 ranks nothing; node ids are only renamed)
+        const u64 m = 2 * N;
         ctx.reserve(ws.w0, m * 8);
         ctx.reserve(ws.w1, m * 8);
-        ctx.reserve(ws.jbuf[0], n * 8);
-        ctx.reserve(ws.jbuf[1], n * 8);
-        const int bits = s.bits;
-        u64 *fw = ws.w0.as<u64>();
-        u64 *rv = wcc ? fw + n : (s.program == DL_PROGRAM_TC ? ws.jbuf[0].as<u64>() : nullptr);
         DL_LAUNCH(ctx, K_PREP, 0,
-                  session_pack_kernel<<<grid_for(n, 256, ctx, 16), 256, 0, ctx.stream>>>(rows, n, gi.ids, (u32) nid,
-                                                                                          in.rank_lo, bits, fw, rv));
-        u64 ne;
-        // tc.cu:171-176, sg.cu:150-153, wcc.cu:140-167: deduplicated edges keyed by source
-        u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, m, 2 * bits, ne);
+                  session_tag_kernel<<<grid_for(N, 256, ctx, 16), 256, 0, ctx.stream>>>(in_rows, N, d_off, (u32) count,
+                                                                                         ws.w0.as<u64>()));
+        u64 nu = 0;
+        u64 *u = sort_unique_into(ctx, ws.w0, ws.w1, m, 32 + bits_for(count), nu);
+        const u64 B = s.next_rank;
+        if (B + nu > s.rank_cap)
+            throw Error(DL_ERR_OVERFLOW, "session node capacity exhausted (" + std::to_string(s.rank_cap) + " ranks)");
+        DevBuf &wu = ws.w0.p == u ? ws.w0 : ws.w1;
+        DevBuf &wo = ws.w0.p == u ? ws.w1 : ws.w0;
+        ctx.reserve(s.admit_first, (count + 1) * 8);
+        DL_LAUNCH(ctx, K_PREP, 0,
+                  session_first_kernel<<<grid_for(count + 1, 256, ctx, 16), 256, 0, ctx.stream>>>(
+                      u, nu, (u32) count, s.admit_first.as<u64>()));
+        std::vector<u64> first(count + 1);
+        DL_CUDA(cudaMemcpyAsync(first.data(), s.admit_first.p, (count + 1) * 8, cudaMemcpyDeviceToHost, ctx.stream));
+        // node ids of the admitted ranks, shared by the instances of this admission
+        auto block = make_block(ctx, nu * 4);
+        DL_LAUNCH(ctx, K_PREP, 0,
+                  session_ids_kernel<<<grid_for(nu, 256, ctx, 16), 256, 0, ctx.stream>>>(u, nu, block->as<int32_t>()));
+        // rows -> rank words; the edge relation keyed by source (tc.cu:171-176,
+        // sg.cu:150-153, wcc.cu:140-167: WCC stores both directions)
+        const int bits = s.bits;
+        const bool wcc = s.program == DL_PROGRAM_WCC, tc = s.program == DL_PROGRAM_TC;
+        if (tc) ctx.reserve(ws.jbuf[0], N * 8);
+        u64 *fw = wo.as<u64>();
+        u64 *rv = wcc ? fw + N : (tc ? ws.jbuf[0].as<u64>() : nullptr);
+        DL_LAUNCH(ctx, K_PREP, 0,
+                  session_pack_many_kernel<<<grid_for(N, 256, ctx, 16), 256, 0, ctx.stream>>>(
+                      in_rows, N, d_off, (u32) count, u, nu, B, bits, fw, rv));
+        u64 ne = 0;
+        u64 *e = sort_unique_into(ctx, wo, wu, wcc ? m : N, 2 * bits, ne);
         if (s.n_vals + ne >= (1ull << 32)) throw Error(DL_ERR_OVERFLOW, "session edge capacity exhausted");
-        grow_keep(ctx, s.off, (in.rank_hi + 1) * 4, (in.rank_lo + 1) * 4);
+        grow_keep(ctx, s.off, (B + nu + 1) * 4, (B + 1) * 4);
         grow_keep(ctx, s.val, (s.n_vals + ne + 1) * 4, s.n_vals * 4);
         DL_LAUNCH(ctx, K_PREP, 0,
-                  session_csr_kernel<<<grid_for(std::max<u64>(ne, nid + 1), 256, ctx, 16), 256, 0, ctx.stream>>>(
-                      e, ne, bits, in.rank_lo, in.rank_hi, s.n_vals, s.off.as<u32>(), s.val.as<u32>()));
+                  session_csr_kernel<<<grid_for(std::max<u64>(ne, nu + 1), 256, ctx, 16), 256, 0, ctx.stream>>>(
+                      e, ne, bits, B, B + nu, s.n_vals, s.off.as<u32>(), s.val.as<u32>()));
         s.n_vals += ne;
-        s.next_rank = in.rank_hi;
-        if (s.program == DL_PROGRAM_TC) {
+        s.next_rank = B + nu;
+        ctx.sync();  // `first` is ready
+        for (u64 k = 0; k < count; ++k) {
+            SessionInstance &in = inst(k);
+            in.rank_lo = B + first[k];
+            in.rank_hi = B + first[k + 1];
+            in.n_ids = (u32) (first[k + 1] - first[k]);
+            in.ids_block = block;
+            in.ids_off = first[k];
+        }
+        std::vector<bool> empty_base(count, false);
+        if (tc) {
             u64 nd;
-            u64 *d = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * bits, nd);  // tc.cu:178-189
+            u64 *d = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], N, 2 * bits, nd);  // tc.cu:178-189
             full_insert_new(s, d, nd);
             delta_append(s, d, nd);
         } else if (s.program == DL_PROGRAM_SG) {
-            // sg.cu:170-217: base rule of this instance, probing the union table
+            // sg.cu:170-217: the base rule of the admitted instances, probing the union table
             Graph g = union_graph(s);
             u64 *selfs = &ctx.ctrl->scalar[30];
             DL_CUDA(cudaMemsetAsync(selfs, 0, 8, ctx.stream));
@@ -658,37 +840,50 @@ i64 session_admit(SessionImpl &s, const int32_t *rows_in, u64 n, bool on_device)
             ctx.sync();
             const u64 nv = nb - ctx.host_scalars[5];  // self pairs sorted to the end
             const u64 nd = nv ? unique_words(ctx, b, nv, b) : 0;
+            std::vector<u64> lo(count);
+            for (u64 k = 0; k < count; ++k) lo[k] = inst(k).rank_lo;
+            const std::vector<u64> c = range_counts(s, b, nd, bits, lo);
+            for (u64 k = 0; k < count; ++k) empty_base[k] = c[k] == 0;
             full_insert_new(s, b, nd);
             delta_append(s, b, nd);
-            if (nd == 0) {  // the loop runs once on an empty delta (sg.cu:244-390)
-                in.deltas.push_back(0);
-                in.n_result = 0;
-                mark_done(s, in);
-                return in.id;
-            }
         } else {  // wcc.cu:211-231: cc(n, n) for every node, all nodes in the first delta
-            grow_keep(ctx, s.label, in.rank_hi * 4, in.rank_lo * 4);
-            grow_keep(ctx, s.flag, in.rank_hi * 4, in.rank_lo * 4);
-            grow_keep(ctx, s.nextl, (in.rank_hi + 1) * 4, 0);
-            grow_keep(ctx, s.delta, (s.n_delta + nid) * 8, s.n_delta * 8);
+            grow_keep(ctx, s.label, (B + nu) * 4, B * 4);
+            grow_keep(ctx, s.flag, (B + nu) * 4, B * 4);
+            grow_keep(ctx, s.nextl, (B + nu + 1) * 4, 0);
+            grow_keep(ctx, s.delta, (s.n_delta + nu) * 8, s.n_delta * 8);
             DL_LAUNCH(ctx, K_PREP, 0,
-                      session_label_init_kernel<<<grid_for(nid, 256, ctx, 16), 256, 0, ctx.stream>>>(
-                          s.label.as<u32>(), s.flag.as<u32>(), in.rank_lo, in.rank_hi,
-                          s.delta.as<u64>() + s.n_delta));
-            s.n_delta += nid;
-            in.prev_delta = (i64) nid;
+                      session_label_init_kernel<<<grid_for(nu, 256, ctx, 16), 256, 0, ctx.stream>>>(
+                          s.label.as<u32>(), s.flag.as<u32>(), B, B + nu, s.delta.as<u64>() + s.n_delta));
+            s.n_delta += nu;
+            for (u64 k = 0; k < count; ++k) inst(k).prev_delta = (i64) inst(k).n_ids;
         }
         ctx.sync();
+        for (u64 k = 0; k < count; ++k) {
+            SessionInstance &in = inst(k);
+            if (nrows[k] == 0) {
+                mark_done(s, in);
+            } else if (empty_base[k]) {  // the loop runs once on an empty delta (sg.cu:244-390)
+                in.deltas.push_back(0);
+                mark_done(s, in);
+            } else {
+                in.active = true;
+                s.active.push_back(in.id);
+            }
+        }
+        s.inst_dirty = true;
     } catch (...) {
-        // the union tables may hold part of this instance; its ranks are never reused
-        in.done = true;
-        in.released = true;
+        // the union tables may hold part of these instances; their ranks are never reused
+        for (u64 k = 0; k < count; ++k) {
+            inst(k).done = true;
+            inst(k).released = true;
+        }
         throw;
     }
-    in.active = true;
-    s.active.push_back(in.id);
-    s.inst_dirty = true;
-    return in.id;
+    return ids;
+}
+
+i64 session_admit(SessionImpl &s, const int32_t *rows, u64 n, bool on_device) {
+    return session_admit_many(s, &rows, &n, 1, on_device)[0];
 }
 
 u64 session_step(SessionImpl &s) {
@@ -753,17 +948,17 @@ void session_copy_output(SessionImpl &s, i64 id, int32_t *dst, u64 capacity, boo
         ctx.reserve(stage, n * 8);
         tmp = stage.as<int32_t>();
     }
-    const int32_t *ids = in.ids.as<int32_t>();
+    const int32_t *ids = in.ids();
     const unsigned g = grid_for(n, 256, ctx, 16);
     if (s.program == DL_PROGRAM_WCC)
-        DL_LAUNCH(ctx, K_PREP, 0, session_unpack_comp_kernel<<<g, 256, 0, ctx.stream>>>(in.result.as<u32>(), n, ids, tmp));
+        DL_LAUNCH(ctx, K_PREP, 0, session_unpack_comp_kernel<<<g, 256, 0, ctx.stream>>>(in.result_u32(), n, ids, tmp));
     else if (s.program == DL_PROGRAM_SG)
         DL_LAUNCH(ctx, K_PREP, 0,
-                  session_unpack_kernel<true><<<g, 256, 0, ctx.stream>>>(in.result.as<u64>(), n, s.bits, in.rank_lo,
+                  session_unpack_kernel<true><<<g, 256, 0, ctx.stream>>>(in.result_words(), n, s.bits, in.rank_lo,
                                                                           ids, tmp));
     else
         DL_LAUNCH(ctx, K_PREP, 0,
-                  session_unpack_kernel<false><<<g, 256, 0, ctx.stream>>>(in.result.as<u64>(), n, s.bits, in.rank_lo,
+                  session_unpack_kernel<false><<<g, 256, 0, ctx.stream>>>(in.result_words(), n, s.bits, in.rank_lo,
                                                                            ids, tmp));
     if (!on_device) DL_CUDA(cudaMemcpyAsync(dst, tmp, n * 8, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
@@ -781,18 +976,18 @@ void session_copy_labels(SessionImpl &s, i64 id, int32_t *node_ids, int32_t *lab
     ctx.reserve(stage, n * 4);
     DL_LAUNCH(ctx, K_PREP, 0,
               session_unpack_labels_kernel<<<grid_for(n, 256, ctx, 16), 256, 0, ctx.stream>>>(
-                  in.labels.as<u32>(), in.rank_lo, n, in.ids.as<int32_t>(), stage.as<int32_t>()));
+                  in.labels(), in.rank_lo, n, in.ids(), stage.as<int32_t>()));
     DL_CUDA(cudaMemcpyAsync(labels, stage.p, n * 4, cudaMemcpyDeviceToHost, ctx.stream));
-    DL_CUDA(cudaMemcpyAsync(node_ids, in.ids.p, n * 4, cudaMemcpyDeviceToHost, ctx.stream));
+    DL_CUDA(cudaMemcpyAsync(node_ids, in.ids(), n * 4, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
     ctx.give_back(stage);
 }
 
 void session_release(SessionImpl &s, i64 id) {
     SessionInstance &in = finished_instance(s, id);
-    s.ctx.give_back(in.result);
-    s.ctx.give_back(in.labels);
-    s.ctx.give_back(in.ids);
+    in.result_block.reset();  // each block goes with its last instance
+    in.labels_block.reset();
+    in.ids_block.reset();
     in.released = true;
 }
 
@@ -803,13 +998,19 @@ u64 session_device_bytes(const SessionImpl &s) {
     const DevBuf *bufs[] = {&s.off,     &s.val,       &s.delta,    &s.label,      &s.flag,       &s.nextl,
                             &w.input,   &w.ids,       &w.w0,       &w.w1,         &w.csr_off,    &w.csr_val,
                             &w.full[0], &w.full[1],   &w.small[0], &w.small[1],   &w.sample,     &w.jbuf[0],
-                            &w.jbuf[1], &w.offsets,   &c.lookback, &c.radix_part, &c.lbs_splits, &c.sort_hist};
+                            &w.jbuf[1], &w.offsets,   &c.lookback, &c.radix_part, &c.lbs_splits, &c.sort_hist,
+                            &c.merge_splits};
     for (const DevBuf *x : bufs) b += x->cap;
     for (const auto &x : c.spares) b += x.cap;
-    for (const auto &in : s.inst) b += in.ids.cap + in.result.cap + in.labels.cap;
+    std::vector<const DevBuf *> blocks;
+    for (const auto &in : s.inst)
+        for (const DevBuf *x : {in.ids_block.get(), in.result_block.get(), in.labels_block.get()})
+            if (x && std::find(blocks.begin(), blocks.end(), x) == blocks.end()) blocks.push_back(x);
+    for (const DevBuf *x : blocks) b += x->cap;
     return b;
 }
 
 u64 session_active(const SessionImpl &s) { return s.active.size(); }
+u64 session_instance_count(const SessionImpl &s) { return s.inst.size(); }
 
 }  // namespace dl

@@ -1,6 +1,8 @@
 // Multi-instance fixpoint session (batched and served forms); see dl_session.cu.
 #pragma once
 
+#include <memory>
+
 #include "dl_internal.h"
 
 namespace dl {
@@ -9,15 +11,24 @@ struct SessionInstance {
     i64 id = 0;
     i64 input_rows = 0;
     u64 rank_lo = 0, rank_hi = 0;  // union ranks [rank_lo, rank_hi) of this instance
-    DevBuf ids;                    // node id of each local rank
+    std::shared_ptr<DevBuf> ids_block;  // node ids of the admission this instance came with
+    u64 ids_off = 0;                    // first local rank's entry in ids_block
     u32 n_ids = 0;
+    const int32_t *ids() const { return ids_block ? ids_block->as<int32_t>() + ids_off : nullptr; }
     std::vector<i64> deltas;       // |delta| of this instance after each iteration
     i64 prev_delta = 0;            // WCC reference stop rule
     bool active = false, done = false, released = false;
-    DevBuf result;                 // TC/SG: sorted union words; WCC: component ranks (local)
+    // TC/SG: sorted union words; WCC: component ranks (local). Instances that
+    // finish in the same step share one block.
+    std::shared_ptr<DevBuf> result_block;
+    u64 result_off = 0;
     u64 n_result = 0;
-    DevBuf labels;                 // WCC: union label rank of every local node
+    std::shared_ptr<DevBuf> labels_block;  // WCC: union label rank of every local node
+    u64 labels_off = 0;
     i64 largest = 0;               // WCC: largest component size
+    const u64 *result_words() const { return result_block->as<u64>() + result_off; }
+    const u32 *result_u32() const { return result_block->as<u32>() + result_off; }
+    const u32 *labels() const { return labels_block->as<u32>() + labels_off; }
 };
 
 struct SessionImpl;
@@ -28,6 +39,10 @@ SessionImpl *session_create(Context &parent, int program, const dl_options &opt,
 void session_destroy(SessionImpl *s);
 // Adds an instance; its first iteration runs with the next session_step.
 i64 session_admit(SessionImpl &s, const int32_t *rows, u64 n, bool on_device);
+// Adds `count` instances at once (one ranking sort and one edge sort for
+// all of them); returns their ids in order.
+std::vector<i64> session_admit_many(SessionImpl &s, const int32_t *const *rows, const u64 *n, u64 count,
+                                    bool on_device);
 // One semi-naive iteration of every active instance; returns how many remain active.
 u64 session_step(SessionImpl &s);
 // Moves up to `capacity` ids of the instances finished since the last poll
@@ -43,5 +58,6 @@ void session_copy_labels(SessionImpl &s, i64 id, int32_t *node_ids, int32_t *lab
 void session_release(SessionImpl &s, i64 id);
 u64 session_device_bytes(const SessionImpl &s);
 u64 session_active(const SessionImpl &s);
+u64 session_instance_count(const SessionImpl &s);
 
 }  // namespace dl

@@ -300,9 +300,13 @@ __global__ void sparse_mark_kernel(const u64 *__restrict__ j, u64 nj, const u64 
 
 u64 *partition(Context &ctx, const u64 *a, u64 na, const u64 *b, u64 nb, Codec codec, u64 &tiles) {
     tiles = (na + nb + MP_TILE - 1) / MP_TILE;
-    // Look-back words of the launch occupy [0, tiles + 1) of the context's
-    // look-back buffer; the split points follow them.
-    u64 *splits = ctx.lookback_words(2 * (tiles + 1)) + (tiles + 1);
+    // The split points get their own buffer: the look-back buffer is cleared
+    // whenever the launch epoch wraps, which may happen at the next launch.
+    if ((tiles + 1) * sizeof(u64) > ctx.merge_splits.cap) {
+        ctx.sync();
+        ctx.merge_splits.reserve((tiles + 1) * sizeof(u64));
+    }
+    u64 *splits = ctx.merge_splits.as<u64>();
     const unsigned grid = (unsigned) ((tiles + 1 + 255) / 256);
     if (codec == Codec::Entity) DL_LAUNCH(ctx, K_MERGE_PARTITION, 0, merge_partition_kernel<true><<<grid, 256, 0, ctx.stream>>>(a, na, b, nb, tiles + 1, splits));
     else DL_LAUNCH(ctx, K_MERGE_PARTITION, 0, merge_partition_kernel<false><<<grid, 256, 0, ctx.stream>>>(a, na, b, nb, tiles + 1, splits));
@@ -359,7 +363,7 @@ u64 diff_merge_words(Context &ctx, const u64 *full, u64 nfull, const u64 *j, u64
     if (nfull + nj == 0) return 0;
     u64 tiles;
     u64 *splits = partition(ctx, full, nfull, j, nj, codec, tiles);
-    u64 *lb = ctx.lookback.as<u64>();  // first tiles+1 words (reserved by partition)
+    u64 *lb = ctx.lookback_words(tiles + 1);
     u32 *ctr = ctx.tile_counter(40);
     u64 *cnt = &ctx.ctrl->scalar[1];
     DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(u32), ctx.stream));

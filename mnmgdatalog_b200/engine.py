@@ -21,6 +21,7 @@ DatalogError. Torch is used for device buffers only.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -107,11 +108,14 @@ class Engine:
         if stream is not None:
             s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
         self._stream_obj = stream
+        self._sessions = weakref.WeakSet()
         check(lib().dl_context_create(device, s, C.byref(h)))
         self.ctx = h
 
     def close(self):
         if getattr(self, "ctx", None):
+            for sess in list(getattr(self, "_sessions", ())):  # sessions hand their memory back first
+                sess.close()
             lib().dl_context_destroy(self.ctx)
             self.ctx = None
 

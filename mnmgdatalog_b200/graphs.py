@@ -93,6 +93,37 @@ def lattice3d(side: int = 55, p: float = 0.15, long_frac: float = 0.01, seed: in
     return _dedup(rows)
 
 
+def sized(program: str, edges: int, seed: int = 0) -> np.ndarray:
+    """An input of about `edges` rows for one program, from the generators
+    above: TC on a DAG (n = edges / 1.1, extra = 0.4 n), SG on a lattice
+    (side = (edges / 0.9)^(1/3)), WCC on a Chung-Lu graph with exponent 2.3
+    (n = edges / 3.3, the node/edge ratio of the TC-at-scale graph)."""
+    if program == "tc":
+        n = max(8, int(edges / 1.1))
+        return dag(n=n, extra=int(0.4 * n), seed=seed)
+    if program == "sg":
+        return lattice3d(side=max(3, int(round((edges / 0.9) ** (1.0 / 3.0)))), seed=seed)
+    if program == "wcc":
+        return chung_lu(n=max(16, int(edges / 3.3)), m=edges, gamma=2.3, seed=seed)
+    raise ValueError(program)
+
+
+def log_uniform(count: int, lo: int, hi: int, rng: np.random.Generator) -> np.ndarray:
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), size=count)).astype(np.int64)
+
+
+def batched_workload(count: int = 1024, lo: int = 1000, hi: int = 200_000, seed: int = 0) -> list:
+    """The batched configuration: half TC on DAGs, half WCC on Chung-Lu
+    graphs (exponent 2.3), edge counts log-uniform in [lo, hi].
+    Returns [(program, edges), ...] with the TC instances first."""
+    rng = np.random.default_rng(seed)
+    sizes = log_uniform(count, lo, hi, rng)
+    half = count // 2
+    out = [("tc", sized("tc", int(sizes[i]), seed=seed * 100_003 + i)) for i in range(half)]
+    out += [("wcc", sized("wcc", int(sizes[i]), seed=seed * 100_003 + i)) for i in range(half, count)]
+    return out
+
+
 CONFIGS = {
     # name: (program, generator, kwargs)
     "c0_tc_dag": ("tc", dag, {}),

@@ -65,6 +65,7 @@ class Session:
             opts = _options(wcc_stop, max_iterations)
             check(lib().dl_session_create(engine.ctx, self._prog, C.byref(opts), max_nodes, C.byref(h)))
             self.handle = h
+        engine._sessions.add(self)
 
     def close(self):
         if getattr(self, "handle", None):
@@ -89,6 +90,23 @@ class Session:
         i = C.c_int64()
         check(lib().dl_session_admit(self.handle, C.c_void_p(ptr) if ptr else None, n, on_dev, C.byref(i)))
         return i.value
+
+    def admit_many(self, edge_sets) -> list[int]:
+        """Adds several instances with one ranking sort and one edge sort;
+        returns their ids (consecutive)."""
+        args = [_edge_arg(e) for e in edge_sets]
+        if not args:
+            return []
+        on_dev = {a[2] for a in args if a[1]}
+        if len(on_dev) > 1:
+            raise DatalogError(1, "edge sets must all be host arrays or all CUDA tensors")
+        count = len(args)
+        ptrs = (C.c_void_p * count)(*[C.c_void_p(a[0]) if a[0] else None for a in args])
+        rows = (C.c_int64 * count)(*[a[1] for a in args])
+        first = C.c_int64()
+        check(lib().dl_session_admit_many(self.handle, ptrs, rows, count, on_dev.pop() if on_dev else 0,
+                                          C.byref(first)))
+        return list(range(first.value, first.value + count))
 
     def step(self) -> int:
         """One iteration of every active instance; returns how many are still active."""
@@ -127,6 +145,8 @@ class Session:
                                            deltas.size))
         nout = info.output_rows
         rows = None
+        if output not in ("host", "device", "none"):
+            raise DatalogError(1, f"output must be host, device or none, not {output!r}")
         if output == "host":
             rows = out[:nout] if out is not None else np.empty((nout, 2), dtype=np.int32)
             check(lib().dl_session_copy_output(self.handle, instance, rows.ctypes.data if nout else None, nout, 0))

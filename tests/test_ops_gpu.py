@@ -121,3 +121,38 @@ def test_skewed_join_hub(engine):
     ht.close()
     assert got.shape == (10_000_000, 2)
     assert np.array_equal(got, ops.join(rel, probe))
+
+
+def test_diff_merge_across_epoch_wrap():
+    """The 14-bit look-back epoch wraps after 16383 launches and the wrap
+    clears the look-back buffer; the merge-path split points of the launch
+    that wraps must survive it. On a fresh context every dl_diff_merge call
+    takes exactly one epoch, so call 16384 is the one that wraps."""
+    import ctypes as C
+
+    import torch
+
+    from mnmgdatalog_b200 import Engine
+    from mnmgdatalog_b200.capi import check, lib
+    rng = np.random.default_rng(5)
+    full = ops.sort_unique(rand_rel(rng, 9000))
+    j = ops.sort(rand_rel(rng, 5000))
+    want_delta = ops.set_difference(ops.sort_unique(j), full)
+    want_full = ops.sort_unique(np.concatenate([full, j]))
+    with Engine(0) as eng:
+        df, dj = T(full), T(j)
+        fo = torch.empty((len(full) + len(j), 2), dtype=torch.int32, device="cuda")
+        do = torch.empty((len(j), 2), dtype=torch.int32, device="cuda")
+        n = C.c_int64()
+        args = (eng.ctx, C.c_void_p(df.data_ptr()), len(full), C.c_void_p(dj.data_ptr()), len(j),
+                C.c_void_p(fo.data_ptr()), C.c_void_p(do.data_ptr()), C.byref(n))
+        torch.cuda.synchronize()
+        for call in range(1, 16400):
+            fo.zero_()
+            eng.synchronize()
+            check(lib().dl_diff_merge(*args))
+            assert n.value == len(want_delta), call
+            if call >= 16380 or call % 4096 == 0:
+                eng.synchronize()
+                assert np.array_equal(H(fo[: len(full) + n.value]), want_full), call
+                assert np.array_equal(H(do[: n.value]), want_delta), call

@@ -176,3 +176,24 @@ def test_session_errors(engine):
         s.admit(np.array([[1, 2], [2, 3]], np.int32))
         with pytest.raises(DatalogError):
             s.admit(np.array([[7, 8], [8, 9]], np.int32))  # 6 nodes > 4
+
+
+@pytest.mark.parametrize("prog", ["tc", "sg", "wcc"])
+def test_admit_many_while_running(engine, prog):
+    """Groups of instances (with empty ones among them) admitted in one call,
+    between steps of the running ones."""
+    inst = _instances(prog, seed=13)
+    plain = [engine.run(prog, e, labels=True) for e in inst]
+    got = {}
+    with engine.session(prog) as s:
+        first = s.admit_many(inst[:5])
+        assert first == list(range(5))
+        s.step()
+        second = s.admit_many(inst[5:])
+        assert second == list(range(5, len(inst)))
+        assert s.admit_many([]) == []
+        s.run()
+        for i in range(len(inst)):
+            got[i] = s.result(i, labels=True)
+    for k, p in enumerate(plain):
+        _same(got[k], p, prog, f"input {k}")
