@@ -262,6 +262,18 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
         except Exception as exc:  # reported in the line, never hidden
             e2e = {"value": None, "unit": UNIT, "error": f"{type(exc).__name__}: {exc}"}
 
+    batched = served = None
+    if args.batch_instances > 0:
+        try:
+            batched = measure_batched(eng, dev, args)
+        except Exception as exc:  # reported in the line, never hidden
+            batched = {"error": f"{type(exc).__name__}: {exc}"}
+    if args.serve_requests > 0:
+        try:
+            served = measure_served(eng, args)
+        except Exception as exc:
+            served = {"error": f"{type(exc).__name__}: {exc}"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -279,7 +291,8 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
                 "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": launches, "clocks": clk, "kernels": kernels, "host": host_costs}
+                "gpu_launches": launches, "clocks": clk, "kernels": kernels, "host": host_costs,
+                "batched": batched, "served": served}
         print(json.dumps(line))
     eng.close()
     return 0
@@ -324,6 +337,95 @@ def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
             "steps": steps, "timer": "host wall clock, synchronized"}
 
 
+def measure_batched(eng, dev, args) -> dict:
+    """The batched form on 1,024 instances (half TC on DAGs, half WCC on
+    Chung-Lu graphs with exponent 2.3, edge counts log-uniform in 1K-200K):
+    dl_run_batch per program against the plain engine run one instance at a
+    time, inputs resident in HBM for both, outputs left on the device."""
+    import torch
+
+    from mnmgdatalog_b200 import graphs
+    work = graphs.batched_workload(count=args.batch_instances, seed=0)
+    groups = {p: [torch.from_numpy(e).to(dev) for q, e in work if q == p] for p in ("tc", "wcc")}
+    torch.cuda.synchronize(dev)
+    for _ in range(max(1, min(args.warmup, 2))):
+        for p, g in groups.items():
+            eng.run_batch(p, g, output="none")
+    eng.synchronize()
+    reps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        batched = {p: eng.run_batch(p, g, output="none") for p, g in groups.items()}
+    eng.synchronize()
+    t_batch = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    plain = {p: [eng.run(p, x, output="none") for x in g] for p, g in groups.items()}
+    eng.synchronize()
+    t_plain = time.perf_counter() - t0
+    same = all(a.iterations == b.iterations and a.output_tuples == b.output_tuples
+               and a.deltas.tolist() == b.deltas.tolist()
+               for p in groups for a, b in zip(batched[p], plain[p]))
+    n = sum(len(g) for g in groups.values())
+    tuples = sum(r.output_tuples for p in ("tc",) for r in plain[p])
+    return {"workload": f"{n} instances: {len(groups['tc'])} TC on DAGs + {len(groups['wcc'])} WCC on Chung-Lu "
+                        f"gamma=2.3, edges log-uniform 1K-200K (seed 0)",
+            "edges_total": int(sum(len(e) for _, e in work)), "tc_tuples": int(tuples),
+            "queries_per_s": n / t_batch, "plain_queries_per_s": n / t_plain,
+            "speedup_vs_plain": t_plain / t_batch, "seconds": t_batch, "plain_seconds": t_plain,
+            "reps": reps, "identical_to_plain": bool(same),
+            "timer": "host wall clock around dl_run_batch per program (synchronized), inputs in HBM",
+            "form": "union fixpoint per program (one launch sequence per iteration for all instances)"}
+
+
+def measure_served(eng, args) -> dict:
+    """The served form: a Poisson stream of mixed TC/SG/WCC requests (edge
+    counts log-uniform in 1K-500K) through the continuous-batching server with
+    a 150 GB HBM budget, against the plain engine serving the same requests
+    one at a time. Capacity is measured with every request queued at t=0;
+    the Poisson run uses 80% of it."""
+    from mnmgdatalog_b200 import serve
+    reqs = serve.mixed_requests(args.serve_requests, lo=1000, hi=500_000, pool=args.serve_pool, seed=0)
+    for r in reqs[:6]:  # warm-up of every program
+        eng.run(r.program, r.edges, output="none")
+    t_plain, svc, _ = serve.serve_plain(eng, reqs, pinned=True, keep_results=False)
+    plain_qps = len(reqs) / t_plain
+
+    def fresh():
+        return [serve.Request(r.id, r.program, r.edges) for r in reqs]
+
+    srv = serve.Server(eng, budget_bytes=150 * 10**9, keep_results=False, concurrent=True, pinned=True)
+    try:
+        sat = srv.serve(fresh())
+    finally:
+        srv.close()
+    rate = 0.8 * sat.queries_per_s
+    stream = fresh()
+    arr = serve.poisson_arrivals(len(stream), rate, np.random.default_rng(1))
+    for r, t in zip(stream, arr):
+        r.arrival = float(t)
+    srv = serve.Server(eng, budget_bytes=150 * 10**9, keep_results=False, concurrent=True, pinned=True)
+    try:
+        poi = srv.serve(stream)
+    finally:
+        srv.close()
+    sp50, sp95, sp99, _ = serve.percentiles(svc)
+    return {"workload": f"{len(reqs)} requests, TC/SG/WCC uniform, edges log-uniform 1K-500K, inputs drawn from "
+                        f"{args.serve_pool} seeded graphs per program, Poisson arrivals at 80% of capacity",
+            "capacity_queries_per_s": sat.queries_per_s, "plain_queries_per_s": plain_qps,
+            "speedup_vs_plain": sat.queries_per_s / plain_qps,
+            "poisson_rate": rate, "poisson_queries_per_s": poi.queries_per_s,
+            "latency_s": {"p50": poi.latency_p50, "p95": poi.latency_p95, "p99": poi.latency_p99,
+                          "max": poi.latency_max},
+            "saturated_latency_s": {"p50": sat.latency_p50, "p95": sat.latency_p95, "p99": sat.latency_p99},
+            "plain_service_s": {"p50": sp50, "p95": sp95, "p99": sp99},
+            "max_active": poi.max_active, "peak_device_bytes": poi.peak_device_bytes,
+            "budget_bytes": poi.budget_bytes, "budget_waits": poi.waits_on_budget,
+            "server": "continuous batching, one union session per program, one worker thread and stream per "
+                      "program",
+            "delivery": "result rows copied into reused page-locked host buffers (served and plain alike)",
+            "timer": "host wall clock; latency = result rows on the host - arrival"}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,6 +435,9 @@ def main(argv=None) -> int:
     ap.add_argument("--config", default="c1_tc_chung_lu")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=1024, help="batched form instances (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=600, help="served form requests (0: skip)")
+    ap.add_argument("--serve-pool", type=int, default=32, help="distinct seeded graphs per program")
     args = ap.parse_args(argv)
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)

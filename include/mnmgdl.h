@@ -217,8 +217,8 @@ DL_API dl_status dl_run_destroy(dl_run *run);
  * must not run concurrently. */
 typedef struct dl_session dl_session;
 
-/* max_nodes bounds the node count of the instances alive at once (TC/SG
- * words then carry 2 * ceil(log2(max_nodes)) bits; 0 = 2^30). */
+/* max_nodes bounds the node count of the instances alive at once
+ * (0 = 2^32 - 1); admitting past it fails with DL_ERR_OVERFLOW. */
 DL_API dl_status dl_session_create(dl_context *ctx, int32_t program, const dl_options *opts, int64_t max_nodes,
                                    dl_session **out);
 /* Adds an instance on `rows` int32 edge pairs; *instance receives its id
@@ -245,7 +245,8 @@ DL_API dl_status dl_session_copy_labels(dl_session *s, int64_t instance, int32_t
                                         int64_t capacity);
 /* Frees a finished instance's result memory (its info stays readable). */
 DL_API dl_status dl_session_release(dl_session *s, int64_t instance);
-/* Device bytes held by the session and the number of active instances. */
+/* Device bytes the session's live buffers and unreleased results hold (its
+ * cache of free buffers not included) and the number of active instances. */
 DL_API dl_status dl_session_memory(const dl_session *s, int64_t *device_bytes, int64_t *active);
 DL_API dl_status dl_session_destroy(dl_session *s);
 /* Batched form: admits `count` edge sets (edges[i] holds rows[i] pairs) and

@@ -222,7 +222,7 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
     ctx.reserve(jout, std::max<u64>(total, 1) * 8);
     if (total == 0) return jout.as<u64>();
     const int key_bits = 2 * g.bits;
-    const bool fuse_hist = radix_wants_histogram();
+    const bool fuse_hist = radix_wants_histogram() && !g.nwin;
     const int ndig = fuse_hist ? (key_bits + 7) / 8 : 0;
     u64 *hist = fuse_hist ? radix_hist_buffer(ctx) : nullptr;
     if (fuse_hist) radix_hist_clear(ctx);
@@ -232,6 +232,7 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
     DevBuf &pbuf = holder(ws, probe);
     u64 *jptr = jout.as<u64>();
     ctx.reserve(pbuf, total * 8);  // probe is dead now
+    if (g.nwin) return radix_sort_windows(ctx, jptr, pbuf.as<u64>(), total, g.win, g.nwin);
     return radix_sort(ctx, jptr, pbuf.as<u64>(), total, Codec::Raw, key_bits, hist);
 }
 

@@ -51,6 +51,9 @@ struct Graph {
     int bits = 1;
     int32_t *ids = nullptr;
     Csr csr;
+    // Radix windows of join-output sorts; 0 = every digit of [0, 2 * bits).
+    int nwin = 0;
+    int win[8] = {};
 };
 
 struct FullSet {

@@ -171,6 +171,14 @@ enum class Codec { Raw = 0, Entity = 1 };
 // digits that vary (one host read). Returns the buffer holding the result.
 u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits,
                 u64 *hist_accumulated = nullptr);
+// Sorts by the 8-bit windows at the given ascending bit shifts (raw words).
+// Correct when every bit outside the windows is the same in all keys;
+// windows may overlap.
+u64 *radix_sort_windows(Context &ctx, u64 *a, u64 *b, u64 n, const int *shifts, int nwin);
+// Fewest 8-bit windows covering the bits that vary in words
+// (hi << field_bits | lo) whose fields are below 2^used_bits; fills shifts
+// (at most 8) and returns their number.
+int plan_windows(int field_bits, int used_bits, int *shifts);
 // Histogram of the digits [0, ndigits) accumulated by producers (join emit)
 // into ctx.sort_hist; lets radix_sort skip its own histogram pass.
 u64 *radix_hist_buffer(Context &ctx);

@@ -450,7 +450,50 @@ void lsd3_pass(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, u32 G, u
               kern<<<G, DS_THREADS, smem, ctx.stream>>>(in, out, n, shift, chunk, G, offs, use_tma, &ctx.ctrl->err));
 }
 
+// CTA count and chunk (a multiple of the tile) of a three-kernel pass over n
+// keys; reserves the per-(digit, CTA) counts.
+void lsd3_grid(Context &ctx, u64 n, u64 &G, u64 &chunk) {
+    G = std::min<u64>((u64) ctx.sm_count * 2, (n + DS_TILE - 1) / DS_TILE);
+    if (G == 0) G = 1;
+    chunk = (n + G - 1) / G;
+    chunk = (chunk + DS_TILE - 1) / DS_TILE * DS_TILE;
+    G = (n + chunk - 1) / chunk;
+    ctx.reserve(ctx.radix_part, 2 * RADIX * G * sizeof(u64));
+}
+
 }  // namespace
+
+u64 *radix_sort_windows(Context &ctx, u64 *a, u64 *b, u64 n, const int *shifts, int nwin) {
+    if (n <= 1 || nwin <= 0) return a;
+    if (!use_lsd3()) return radix_sort(ctx, a, b, n, Codec::Raw, shifts[nwin - 1] + 8);
+    u64 G, chunk;
+    lsd3_grid(ctx, n, G, chunk);
+    u64 *ph = ctx.radix_part.as<u64>();
+    u64 *po = ph + RADIX * G;
+    const u64 *src = a;
+    u64 *dst = b;
+    for (int p = 0; p < nwin; ++p) {
+        lsd3_pass<false, false>(ctx, src, dst, n, shifts[p], (u32) G, chunk, ph, po);
+        u64 *t = const_cast<u64 *>(src);
+        src = dst;
+        dst = t;
+    }
+    return const_cast<u64 *>(src);
+}
+
+int plan_windows(int field_bits, int used_bits, int *shifts) {
+    const int B = field_bits, kb = std::max(1, std::min(used_bits, field_bits));
+    const int per_field = (kb + 7) / 8;
+    const int contiguous = (B + kb + 7) / 8;
+    int n = 0;
+    if (contiguous <= 2 * per_field) {
+        for (int i = 0; i < contiguous; ++i) shifts[n++] = 8 * i;
+    } else {
+        for (int i = 0; i < per_field; ++i) shifts[n++] = 8 * i;
+        for (int i = 0; i < per_field; ++i) shifts[n++] = B + 8 * i;
+    }
+    return n;
+}
 
 // Histogram bins [8][256] followed by bucket bases [8][256].
 u64 *radix_hist_buffer(Context &ctx) {
@@ -503,12 +546,8 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
     const u64 *src = a;
     u64 *dst = b;
     if (lsd3) {
-        u64 G = std::min<u64>((u64) ctx.sm_count * 2, (n + DS_TILE - 1) / DS_TILE);
-        if (G == 0) G = 1;
-        u64 chunk = (n + G - 1) / G;
-        chunk = (chunk + DS_TILE - 1) / DS_TILE * DS_TILE;
-        G = (n + chunk - 1) / chunk;
-        ctx.reserve(ctx.radix_part, 2 * RADIX * G * sizeof(u64));
+        u64 G, chunk;
+        lsd3_grid(ctx, n, G, chunk);
         u64 *ph = ctx.radix_part.as<u64>();
         u64 *po = ph + RADIX * G;
         for (int p = 0; p < nd; ++p) {

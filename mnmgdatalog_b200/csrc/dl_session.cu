@@ -317,7 +317,20 @@ Graph union_graph(SessionImpl &s) {
     g.csr.val = s.val.as<u32>();
     g.csr.n_keys = (u32) s.next_rank;
     g.csr.n_vals = s.n_vals;
+    // both rank fields are below next_rank: sort only the bits that can vary
+    g.nwin = plan_windows(s.bits, bits_for(std::max<u64>(s.next_rank, 2)), g.win);
     return g;
+}
+
+// Sorts the n words of buf (alt: ping-pong) whose rank fields are below
+// 2^used_bits and drops duplicates.
+u64 *sort_unique_fields(Context &ctx, DevBuf &buf, DevBuf &alt, u64 n, int field_bits, int used_bits, u64 &n_out) {
+    ctx.reserve(alt, std::max<u64>(n, 1) * 8);
+    int w[8];
+    const int nw = plan_windows(field_bits, used_bits, w);
+    u64 *r = radix_sort_windows(ctx, buf.as<u64>(), alt.as<u64>(), n, w, nw);
+    n_out = unique_words(ctx, r, n, r);
+    return r;
 }
 
 // Inserts the words of a brand-new key range into the full relation.
@@ -682,10 +695,11 @@ SessionImpl *session_create(Context &parent, int program, const dl_options &opt,
         s->bits = 32;
         s->rank_cap = 0xFFFFFFFFull;
     } else {
-        // TC/SG words hold two ranks; fewer bits mean fewer radix passes
-        s->bits = max_nodes ? std::max(1, bits_for(max_nodes)) : 30;
-        if (s->bits > 31) throw Error(DL_ERR_INVALID_ARGUMENT, "max_nodes above 2^31");
-        s->rank_cap = 1ull << s->bits;
+        // TC/SG words hold two rank fields of `bits` bits; the sorts only
+        // visit the bits the ranks in use can set
+        s->bits = max_nodes ? std::max(1, bits_for(max_nodes)) : 32;
+        if (max_nodes >= 0xFFFFFFFFull) throw Error(DL_ERR_INVALID_ARGUMENT, "max_nodes above 2^32 - 2");
+        s->rank_cap = s->bits == 32 ? 0xFFFFFFFFull : (1ull << s->bits);
     }
     Context &c = s->ctx;
     s->parent = &parent;
@@ -804,7 +818,8 @@ std::vector<i64> session_admit_many(SessionImpl &s, const int32_t *const *rows, 
                   session_pack_many_kernel<<<grid_for(N, 256, ctx, 16), 256, 0, ctx.stream>>>(
                       in_rows, N, d_off, (u32) count, u, nu, B, bits, fw, rv));
         u64 ne = 0;
-        u64 *e = sort_unique_into(ctx, wo, wu, wcc ? m : N, 2 * bits, ne);
+        const int used = bits_for(std::max<u64>(B + nu, 2));
+        u64 *e = sort_unique_fields(ctx, wo, wu, wcc ? m : N, bits, used, ne);
         if (s.n_vals + ne >= (1ull << 32)) throw Error(DL_ERR_OVERFLOW, "session edge capacity exhausted");
         grow_keep(ctx, s.off, (B + nu + 1) * 4, (B + 1) * 4);
         grow_keep(ctx, s.val, (s.n_vals + ne + 1) * 4, s.n_vals * 4);
@@ -825,7 +840,7 @@ std::vector<i64> session_admit_many(SessionImpl &s, const int32_t *const *rows, 
         std::vector<bool> empty_base(count, false);
         if (tc) {
             u64 nd;
-            u64 *d = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], N, 2 * bits, nd);  // tc.cu:178-189
+            u64 *d = sort_unique_fields(ctx, ws.jbuf[0], ws.jbuf[1], N, bits, used, nd);  // tc.cu:178-189
             full_insert_new(s, d, nd);
             delta_append(s, d, nd);
         } else if (s.program == DL_PROGRAM_SG) {
@@ -1000,8 +1015,7 @@ u64 session_device_bytes(const SessionImpl &s) {
                             &w.full[0], &w.full[1],   &w.small[0], &w.small[1],   &w.sample,     &w.jbuf[0],
                             &w.jbuf[1], &w.offsets,   &c.lookback, &c.radix_part, &c.lbs_splits, &c.sort_hist,
                             &c.merge_splits};
-    for (const DevBuf *x : bufs) b += x->cap;
-    for (const auto &x : c.spares) b += x.cap;
+    for (const DevBuf *x : bufs) b += x->cap;  // cached spare buffers are not counted: they are free memory
     std::vector<const DevBuf *> blocks;
     for (const auto &in : s.inst)
         for (const DevBuf *x : {in.ids_block.get(), in.result_block.get(), in.labels_block.get()})

@@ -153,7 +153,8 @@ class Engine:
         """Run one program. `edges` is an (n, 2) int32 host array or a CUDA
         tensor (then the input stays on the device). `output` is "host"
         (numpy), "device" (torch tensor) or "none"; `out` optionally supplies
-        the (capacity, 2) int32 destination (e.g. pinned host memory)."""
+        the (capacity, 2) int32 destination (e.g. pinned host memory), or a
+        callable that returns one for the result's row count."""
         torch = _torch()
         prog = PROGRAMS[program]
         opts = capi.dl_options()
@@ -179,6 +180,8 @@ class Engine:
             check(lib().dl_run_copy_iteration_stats(run, jr.ctypes.data, fr.ctypes.data, jr.size))
             nout = info.output_rows
             rows = None
+            if callable(out):
+                out = out(nout)  # a buffer of at least nout rows, or None
             if output == "host":
                 if out is not None:
                     if len(out) < nout or out.dtype != np.int32 or not out.flags.c_contiguous:

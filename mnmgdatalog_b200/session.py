@@ -137,7 +137,9 @@ class Session:
         return info
 
     def result(self, instance: int, *, output: str = "host", labels: bool = False, out=None):
-        """RunResult of a finished instance (rows in the reference's file order)."""
+        """RunResult of a finished instance (rows in the reference's file order).
+        `out` optionally supplies the destination rows, or a callable that
+        returns one for the result's row count."""
         from .engine import RunResult, _torch
         info = self.info(instance)
         deltas = np.zeros(max(info.iterations, 0), dtype=np.int64)
@@ -145,6 +147,8 @@ class Session:
                                            deltas.size))
         nout = info.output_rows
         rows = None
+        if callable(out):
+            out = out(nout)  # a buffer of at least nout rows, or None
         if output not in ("host", "device", "none"):
             raise DatalogError(1, f"output must be host, device or none, not {output!r}")
         if output == "host":

@@ -37,6 +37,9 @@ class FakeSession:
             self.active[i] = len(edges) % 4 + 1
         return i
 
+    def admit_many(self, edge_sets):
+        return [self.admit(e) for e in edge_sets]
+
     def step(self):
         time.sleep(0.001)  # an iteration takes device time
         for i in list(self.active):
@@ -50,7 +53,7 @@ class FakeSession:
         d, self.done = self.done, []
         return d
 
-    def result(self, i):
+    def result(self, i, output="host", out=None):
         e = self.inst[i]
         return FakeResult(np.sort(e, axis=0), len(e) % 4 + 1)
 
@@ -142,3 +145,39 @@ def test_poisson_arrivals_rate():
 def test_percentiles():
     p50, p95, p99, mx = serve.percentiles(list(np.arange(1, 101, dtype=float)))
     assert (p50, mx) == (50.5, 100.0) and 95 <= p95 <= 96 and 99 <= p99 <= 100
+
+
+def test_concurrent_workers_complete_with_their_own_results():
+    log = []
+    srv = _server(log, concurrent=True)
+    reqs = _requests(90, seed=5, spacing=0.0005)
+    st = srv.serve(reqs)
+    assert st.requests == 90 and len(srv.finished) == 90
+    for r in reqs:
+        assert r.done >= r.admitted >= r.arrival >= 0
+        assert np.array_equal(r.result.rows, np.sort(r.edges, axis=0))
+    assert st.max_active > 1
+
+
+def test_concurrent_budget_and_order():
+    log = []
+    srv = _server(log, concurrent=True, budget_bytes=(1 << 20) + 10)
+    srv.row_bytes = {p: 0.0 for p in serve.PROGRAMS}
+    reqs = _requests(24, seed=6)
+    st = srv.serve(reqs)
+    assert st.max_active <= 1 and st.waits_on_budget > 0
+    order = sorted(reqs, key=lambda r: r.admitted)
+    assert [r.id for r in order] == sorted(r.id for r in reqs)
+
+
+def test_concurrent_worker_error_surfaces():
+    import pytest
+
+    class Broken(FakeSession):
+        def step(self):
+            raise RuntimeError("device lost")
+
+    backend = {p: (lambda: Broken([])) for p in serve.PROGRAMS}
+    srv = serve.Server(backend=backend, concurrent=True)
+    with pytest.raises(RuntimeError, match="device lost"):
+        srv.serve(_requests(6, seed=7))

@@ -19,12 +19,13 @@ def _check(engine, reqs):
         assert np.array_equal(got.rows, alone.rows), r.id
 
 
-def test_served_results_equal_alone(engine):
+@pytest.mark.parametrize("concurrent", [False, True], ids=["one_thread", "worker_per_program"])
+def test_served_results_equal_alone(engine, concurrent):
     reqs = serve.mixed_requests(90, lo=40, hi=6000, pool=10, seed=1)
     arr = serve.poisson_arrivals(len(reqs), 600.0, np.random.default_rng(2))
     for r, t in zip(reqs, arr):
         r.arrival = float(t)
-    srv = serve.Server(engine)
+    srv = serve.Server(engine, concurrent=concurrent)
     try:
         st = srv.serve(reqs)
     finally:
@@ -35,9 +36,10 @@ def test_served_results_equal_alone(engine):
     _check(engine, reqs)
 
 
-def test_served_under_tight_budget(engine):
+@pytest.mark.parametrize("concurrent", [False, True], ids=["one_thread", "worker_per_program"])
+def test_served_under_tight_budget(engine, concurrent):
     reqs = serve.mixed_requests(24, lo=40, hi=3000, pool=6, seed=3)
-    srv = serve.Server(engine, budget_bytes=4 << 20)  # below the sum of the estimates
+    srv = serve.Server(engine, budget_bytes=4 << 20, concurrent=concurrent)  # below the sum of the estimates
     try:
         st = srv.serve(reqs)
     finally:
