@@ -59,7 +59,8 @@ def workload(config: str):
 def describe(config: str, edges: np.ndarray) -> dict:
     d = {"c1_tc_chung_lu": "TC, Chung-Lu n=317000 gamma=2.5 m=1050000 (each edge once, seed 0)",
          "c0_tc_dag": "TC, DAG n=5000 p=0.7 + 2000 short edges (seed 0)",
-         "c2_sg_lattice": "SG, 55^3 lattice 6-neighbour p=0.15 + 1% long edges (seed 0)"}
+         "c2_sg_lattice": "SG, 55^3 lattice 6-neighbour p=0.15 + 1% long edges (seed 0)",
+         "p1_tc_chung_lu_small": "TC, Chung-Lu n=40000 gamma=2.5 m=132500 (each edge once, seed 0)"}
     return {"workload": d.get(config, config), "config": config, "input_rows": int(len(edges))}
 
 
@@ -250,7 +251,7 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
                 "traffic": traffic, "launches": dom["timed_launches"],
                 "share_of_step": dom["seconds"] / (my_ms / 1e3),
                 "algorithmic_bytes_per_launch": dom["bytes"] / max(dom["timed_launches"], 1)}
-    kernels = {k: {"launches": v["launches"], "ms": round(1e3 * v["seconds"], 3),
+    kernels = {k: {"launches": v["launches"], "ms": round(1e3 * v["seconds"], 3), "bytes": v["bytes"],
                    "GBps": round(v["bytes"] / v["seconds"] / 1e9, 1) if v["seconds"] else None}
                for k, v in prof.items() if v["launches"]}
     host_costs = {k: {"calls": v["launches"], "ms": round(1e3 * v["seconds"], 3)} for k, v in host.items()}

@@ -21,9 +21,13 @@
 namespace dl {
 namespace {
 
-constexpr int MP_THREADS = 512;
+// 2048-word tiles of 256 threads: six tiles per SM overlap each other's
+// load, search and store phases (the per-tile work between the loads and
+// the stores otherwise leaves the memory pipe idle).
+constexpr int MP_THREADS = 256;
 constexpr int MP_VT = 8;
 constexpr int MP_TILE = MP_THREADS * MP_VT;
+constexpr int MP_BLOCKS_PER_SM = 1536 / MP_THREADS;
 
 template <bool ENC>
 __device__ __forceinline__ u64 ld_enc(const u64 *p) {
@@ -83,35 +87,27 @@ __device__ __forceinline__ void load_tile(MpSmem &s, const u64 *a, u64 a0, u32 l
     }
 }
 
-// Shared memory of diff_merge: the tile's slice of full (a), a staging
-// buffer (first the slice of J, then the full' output), and the insertion
-// index of every new J word.
+// Shared memory of diff_merge: the tile's slices of full and J (then the
+// tile's full' output) and the tile's new J words.
 struct DmSmem {
-    u64 a[MP_TILE];
-    u64 stage[MP_TILE];
-    uint16_t ins[MP_TILE];
+    u64 buf[MP_TILE];
+    u64 dst[MP_TILE];
     u32 scratch[MP_THREADS / 32 + 1];
     u32 tile;
+    u32 has_prev;
+    u64 prev;
     LookbackScratch lbs;
 };
 
-// Number of entries of the sorted list ins[lo, n) that are <= x.
-__device__ __forceinline__ u32 upper_in(const uint16_t *ins, u32 lo, u32 n, u32 x) {
-    u32 hi = n;
-    while (lo < hi) {
-        const u32 mid = (lo + hi) >> 1;
-        if (ins[mid] <= x) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// Shift-copy form of the fused step: only J words are searched (binary
-// search of the tile's full slice); a full word's output position is its
-// index plus the number of new J words inserted before it, so full words
-// are moved without per-word merge logic.
+// The fused step as a balanced merge: every thread takes MP_VT consecutive
+// positions of merge(full, J) (ties take the full word first), so a J word is
+// a duplicate exactly when it equals the merged word before it. Kept words
+// form full' = full u J, the J words among them form delta = J \ full
+// deduplicated. One packed block scan gives both output offsets within the
+// tile; only the delta count needs the decoupled look-back, since the tile's
+// full' offset is its full offset plus the delta words before it.
 template <bool ENC, bool WRITE_FULL, bool WRITE_DELTA>
-__global__ void __launch_bounds__(MP_THREADS, 3)
+__global__ void __launch_bounds__(MP_THREADS, MP_BLOCKS_PER_SM)
 diff_merge_kernel(const u64 *__restrict__ full, u64 nfull, const u64 *__restrict__ jw, u64 nj,
                   const u64 *__restrict__ splits, u64 *__restrict__ full_out, u64 *__restrict__ delta_out,
                   u64 *lb, u32 *tile_ctr, u32 epoch, u32 *err, u64 *delta_count) {
@@ -126,53 +122,69 @@ diff_merge_kernel(const u64 *__restrict__ full, u64 nfull, const u64 *__restrict
     const u64 d1 = min(d0 + MP_TILE, total);
     const u64 a0 = splits[tile], a1 = splits[tile + 1];
     const u64 b0 = d0 - a0, b1 = d1 - a1;
-    const u32 la = (u32) (a1 - a0), lbn = (u32) (b1 - b0);
+    const u32 la = (u32) (a1 - a0), lbn = (u32) (b1 - b0), n = la + lbn;
 #pragma unroll
     for (int k = 0; k < MP_VT; ++k) {
         const u32 i = k * MP_THREADS + tid;
-        if (i < la) s.a[i] = ld_enc<ENC>(full + a0 + i);
-        if (i < lbn) s.stage[i] = ld_enc<ENC>(jw + b0 + i);
+        if (i < n) s.buf[i] = (i < la) ? ld_enc<ENC>(full + a0 + i) : ld_enc<ENC>(jw + b0 + (i - la));
+    }
+    if (tid == 0) {  // the merged word just before the tile: the larger of the two predecessors
+        u64 p = 0;
+        u32 hp = 0;
+        if (a0 > 0) {
+            p = ld_enc<ENC>(full + a0 - 1);
+            hp = 1;
+        }
+        if (b0 > 0) {
+            const u64 q = ld_enc<ENC>(jw + b0 - 1);
+            if (!hp || q > p) p = q;
+            hp = 1;
+        }
+        s.prev = p;
+        s.has_prev = hp;
     }
     __syncthreads();
-
-    // J words: blocked, MP_VT consecutive words per thread.
-    const u32 jb = (u32) tid * MP_VT;
-    u64 bv[MP_VT];
-    uint16_t bp[MP_VT];
-    u32 is_new = 0;
-    {
-        u64 prev = 0;
-        bool hp = false;
-        if (jb > 0 && jb <= lbn) { prev = s.stage[jb - 1]; hp = true; }
-        else if (jb == 0 && b0 > 0) { prev = ld_enc<ENC>(jw + b0 - 1); hp = true; }
-        const bool has_a_before = a0 > 0;
-        const u64 a_before = has_a_before ? ld_enc<ENC>(full + a0 - 1) : 0ull;
-        u32 lo = 0;
+    const u64 *sa = s.buf, *sb = s.buf + la;
+    const u32 diag = min((u32) tid * MP_VT, n);
+    u32 ta = merge_path_smem(sa, la, sb, lbn, diag);
+    u32 tb = diag - ta;
+    u64 last;
+    bool hl;
+    if (diag == 0) {
+        last = s.prev;
+        hl = s.has_prev != 0;
+    } else {
+        const u64 xa = ta > 0 ? sa[ta - 1] : 0ull, xb = tb > 0 ? sb[tb - 1] : 0ull;
+        last = (ta > 0 && (tb == 0 || xa >= xb)) ? xa : xb;
+        hl = true;
+    }
+    u64 val[MP_VT];
+    u32 keep = 0, isnew = 0;
 #pragma unroll
-        for (int k = 0; k < MP_VT; ++k) {
-            bv[k] = 0;
-            bp[k] = 0;
-            if (jb + k < lbn) {
-                const u64 b = s.stage[jb + k];
-                u32 l = lo, h = la;  // lower bound of b in a[lo, la)
-                while (l < h) {
-                    const u32 mid = (l + h) >> 1;
-                    if (s.a[mid] < b) l = mid + 1;
-                    else h = mid;
+    for (int k = 0; k < MP_VT; ++k) {
+        val[k] = 0;
+        if (diag + k < n) {
+            const bool take_a = ta < la && (tb >= lbn || sa[ta] <= sb[tb]);
+            const u64 v = take_a ? sa[ta] : sb[tb];
+            if (take_a) {
+                ++ta;
+                keep |= 1u << k;
+            } else {
+                ++tb;
+                if (!hl || v != last) {
+                    keep |= 1u << k;
+                    isnew |= 1u << k;
                 }
-                lo = l;
-                const bool dup_a = (l < la && s.a[l] == b) || (l == 0 && has_a_before && a_before == b);
-                const bool dup_b = hp && prev == b;
-                if (!dup_a && !dup_b) is_new |= 1u << k;
-                bv[k] = b;
-                bp[k] = (uint16_t) l;
-                prev = b;
-                hp = true;
             }
+            val[k] = v;
+            last = v;
+            hl = true;
         }
     }
-    u32 tile_new;
-    const u32 new_before = block_exclusive_sum<MP_THREADS / 32>((u32) __popc(is_new), s.scratch, &tile_new);
+    u32 tot;
+    const u32 ex = block_exclusive_sum<MP_THREADS / 32>((u32) __popc(keep) | ((u32) __popc(isnew) << 16), s.scratch,
+                                                        &tot);
+    const u32 tile_keep = tot & 0xFFFFu, tile_new = tot >> 16;
     u64 excl = 0;
     if (tile == 0) {
         if (tid == 0) st_relaxed_u64(lb, lb_word(kStatusInc, epoch, tile_new));
@@ -181,49 +193,29 @@ diff_merge_kernel(const u64 *__restrict__ full, u64 nfull, const u64 *__restrict
         excl = lookback_block<MP_THREADS / 32>(lb, tile, epoch, err, s.lbs);
         if (tid == 0) st_relaxed_u64(lb + tile, lb_word(kStatusInc, epoch, excl + tile_new));
     }
-    __syncthreads();  // J slice in s.stage no longer read
+    __syncthreads();  // every thread is done reading the input slices
     {
-        u32 r = new_before;
+        u32 r = ex & 0xFFFFu, q = ex >> 16;
 #pragma unroll
         for (int k = 0; k < MP_VT; ++k) {
-            if ((is_new >> k) & 1u) {
-                s.ins[r] = bp[k];
-                if (WRITE_FULL) s.stage[bp[k] + r] = bv[k];
-                ++r;
-            }
+            if (WRITE_FULL && ((keep >> k) & 1u)) s.buf[r++] = val[k];
+            if (WRITE_DELTA && ((isnew >> k) & 1u)) s.dst[q++] = val[k];
         }
     }
     __syncthreads();
     if (WRITE_FULL) {
-        // full words, striped: position = index + new J words inserted at or before it
-        const u32 lane = tid & 31;
-        u32 c = 0;
-        for (u32 base = (tid & ~31u); base < la; base += MP_THREADS) {
-            const u32 i = base + lane;
-            c = upper_in(s.ins, c, tile_new, base);  // warp-uniform start
-            u32 ci = c;
-            while (ci < tile_new && s.ins[ci] <= i) ++ci;
-            if (i < la) s.stage[i + ci] = s.a[i];
-        }
-        __syncthreads();
-        const u32 nout = la + tile_new;
-        u64 *dst = full_out + a0 + excl;
-        for (u32 i = tid; i < nout; i += MP_THREADS) dst[i] = ENC ? entity_decode(s.stage[i]) : s.stage[i];
+        u64 *out = full_out + a0 + excl;
+        for (u32 i = tid; i < tile_keep; i += MP_THREADS) out[i] = ENC ? entity_decode(s.buf[i]) : s.buf[i];
     }
     if (WRITE_DELTA) {
-        u32 r = new_before;
-#pragma unroll
-        for (int k = 0; k < MP_VT; ++k)
-            if ((is_new >> k) & 1u) s.a[r++] = bv[k];  // a slice consumed above
-        __syncthreads();
-        u64 *dst = delta_out + excl;
-        for (u32 i = tid; i < tile_new; i += MP_THREADS) dst[i] = ENC ? entity_decode(s.a[i]) : s.a[i];
+        u64 *out = delta_out + excl;
+        for (u32 i = tid; i < tile_new; i += MP_THREADS) out[i] = ENC ? entity_decode(s.dst[i]) : s.dst[i];
     }
     if (d1 == total && tid == 0) *delta_count = excl + tile_new;
 }
 
 template <bool ENC>
-__global__ void __launch_bounds__(MP_THREADS, 3)
+__global__ void __launch_bounds__(MP_THREADS, MP_BLOCKS_PER_SM)
 merge_kernel(const u64 *__restrict__ a, u64 na, const u64 *__restrict__ b, u64 nb, const u64 *__restrict__ splits,
              u64 *__restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -129,6 +129,9 @@ CONFIGS = {
     "c0_tc_dag": ("tc", dag, {}),
     "c1_tc_chung_lu": ("tc", chung_lu, {}),
     "c2_sg_lattice": ("sg", lattice3d, {}),
+    # the TC-at-scale shape at 1/8 of the nodes (~3e7 closure tuples, a few
+    # hundred MB: larger than L2, small enough for detailed counter captures)
+    "p1_tc_chung_lu_small": ("tc", chung_lu, {"n": 40_000, "m": 132_500}),
 }
 
 
