@@ -230,13 +230,8 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
     prof = eng.profile_read()
     eng.profile(False)
     my_ms = sum(a.elapsed_time(b) for a, b in evs)
-    t = torch.tensor([my_ms], dtype=torch.float64, device=dev)
-    tot = torch.tensor([float(tuples)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    max_ms = float(t.item())
-    value = float(tot.item()) / (max_ms / 1e3)
+    max_ms, total = combine_ranks(my_ms, float(tuples), world, dev)
+    value = total / (max_ms / 1e3)
 
     # dominant kernel class by device time over the timed region
     peak, peak_kind = measured_peak_gbs()
@@ -313,7 +308,6 @@ def traffic_per_launch(kernel: str, stat: dict):
 
 def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
     import torch
-    import torch.distributed as dist
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
     probe = eng.run(prog, h_edges, output="none")
     out_rows = probe.output_tuples
@@ -328,14 +322,26 @@ def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
         tuples += r.output_tuples
     torch.cuda.synchronize(dev)
     sec = time.perf_counter() - t0
-    t = torch.tensor([sec], dtype=torch.float64, device=dev)
-    tot = torch.tensor([float(tuples)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    return {"value": float(tot.item()) / float(t.item()), "unit": UNIT,
+    sec, total = combine_ranks(sec, float(tuples), world, dev)
+    return {"value": total / sec, "unit": UNIT,
             "h2d_bytes_per_step": int(edges.nbytes), "d2h_bytes_per_step": int(out_rows * 8),
             "steps": steps, "timer": "host wall clock, synchronized"}
+
+
+def combine_ranks(seconds: float, units: float, world: int, device=None) -> tuple[float, float]:
+    """Whole-job timing over the ranks: the slowest rank's time and the sum
+    of the units every rank processed. Every rank must call it (a collective
+    when world > 1); `device` is the tensor device of the process group's
+    backend (a CUDA device for NCCL, None for gloo)."""
+    if world <= 1:
+        return seconds, units
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    u = torch.tensor([units], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
 
 
 def measure_batched(eng, dev, args) -> dict:
