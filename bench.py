@@ -200,7 +200,7 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
             dist.barrier()
 
     def step():
-        return eng.run(prog, d_edges, output="none")
+        return eng.run(prog, d_edges, output="none", dedup=args.dedup)
 
     for _ in range(args.warmup):
         step()
@@ -309,7 +309,7 @@ def traffic_per_launch(kernel: str, stat: dict):
 def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
     import torch
     h_edges = torch.from_numpy(edges).pin_memory().numpy()
-    probe = eng.run(prog, h_edges, output="none")
+    probe = eng.run(prog, h_edges, output="none", dedup=args.dedup)
     out_rows = probe.output_tuples
     out = torch.empty((out_rows, 2), dtype=torch.int32).pin_memory().numpy()
     steps = max(1, min(args.steps, 3))
@@ -318,7 +318,7 @@ def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
     t0 = time.perf_counter()
     tuples = 0
     for _ in range(steps):
-        r = eng.run(prog, h_edges, output="host", out=out)
+        r = eng.run(prog, h_edges, output="host", out=out, dedup=args.dedup)
         tuples += r.output_tuples
     torch.cuda.synchronize(dev)
     sec = time.perf_counter() - t0
@@ -442,6 +442,8 @@ def main(argv=None) -> int:
     ap.add_argument("--config", default="c1_tc_chung_lu")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dedup", choices=["auto", "sort", "hash"], default="auto",
+                    help="how TC removes known tuples (same results)")
     ap.add_argument("--batch-instances", type=int, default=1024, help="batched form instances (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=600, help="served form requests (0: skip)")
     ap.add_argument("--serve-pool", type=int, default=32, help="distinct seeded graphs per program")

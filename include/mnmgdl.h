@@ -76,11 +76,21 @@ typedef enum dl_wcc_stop {
     DL_WCC_STOP_FIXPOINT = 1
 } dl_wcc_stop;
 
+/* How TC removes known tuples from a join output (same results either way). */
+typedef enum dl_dedup {
+    DL_DEDUP_AUTO = 0,  /* the engine's choice (currently SORT) */
+    DL_DEDUP_SORT = 1,  /* radix sort of the join output + merge-path difference against sorted full */
+    DL_DEDUP_HASH = 2   /* full as a hash set of tuple words; one sort of the result at the end
+                           (no per-iteration sort, but random-access bound: 1.7x slower on
+                           the 1.9e9-tuple TC benchmark) */
+} dl_dedup;
+
 typedef struct dl_options {
     int32_t wcc_stop;        /* dl_wcc_stop */
     int32_t max_iterations;  /* 0 = run to the fixpoint */
     int32_t phase_timing;    /* 1 = record per-phase device times (adds events) */
-    int32_t reserved[5];
+    int32_t dedup;           /* dl_dedup (TC runs; SG and sessions always sort) */
+    int32_t reserved[4];
 } dl_options;
 
 typedef struct dl_run_info {

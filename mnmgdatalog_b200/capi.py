@@ -20,6 +20,7 @@ STATUS_NAMES = {
 
 PROGRAM_TC, PROGRAM_SG, PROGRAM_WCC, PROGRAM_SINGLE_JOIN = 0, 1, 2, 3
 WCC_STOP_REFERENCE, WCC_STOP_FIXPOINT = 0, 1
+DEDUP_AUTO, DEDUP_SORT, DEDUP_HASH = 0, 1, 2
 
 # Every symbol include/mnmgdl.h declares (checked by the CPU test suite).
 EXPORTS = (
@@ -48,7 +49,7 @@ class DatalogError(RuntimeError):
 
 class dl_options(C.Structure):
     _fields_ = [("wcc_stop", C.c_int32), ("max_iterations", C.c_int32), ("phase_timing", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("dedup", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class dl_run_info(C.Structure):

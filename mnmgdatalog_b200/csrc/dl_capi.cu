@@ -367,6 +367,7 @@ DL_API dl_status dl_run_program(dl_context *ctx, int32_t program, const int32_t 
     dl_options o{};
     if (opts) o = *opts;
     DL_REQUIRE(o.wcc_stop == DL_WCC_STOP_REFERENCE || o.wcc_stop == DL_WCC_STOP_FIXPOINT, "unknown wcc_stop");
+    DL_REQUIRE(o.dedup >= DL_DEDUP_AUTO && o.dedup <= DL_DEDUP_HASH, "unknown dedup mode");
     auto run = std::make_unique<dl_run>();
     dl_status st = guarded([&] {
         set_device(ctx);
@@ -455,6 +456,7 @@ DL_API dl_status dl_session_create(dl_context *ctx, int32_t program, const dl_op
     dl_options o{};
     if (opts) o = *opts;
     DL_REQUIRE(o.wcc_stop == DL_WCC_STOP_REFERENCE || o.wcc_stop == DL_WCC_STOP_FIXPOINT, "unknown wcc_stop");
+    DL_REQUIRE(o.dedup >= DL_DEDUP_AUTO && o.dedup <= DL_DEDUP_HASH, "unknown dedup mode");
     auto s = std::make_unique<dl_session>();
     s->ctx = ctx;
     dl_status st = guarded([&] {

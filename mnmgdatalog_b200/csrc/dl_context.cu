@@ -145,6 +145,7 @@ void Context::check_device_error() {
         DL_CUDA(cudaMemsetAsync(&ctrl->err, 0, sizeof(u32), stream));
         DL_CUDA(cudaStreamSynchronize(stream));
         reinterpret_cast<volatile u32 *>(host_scalars)[2 * 63] = 0;
+        if (err & DL_DEVERR_HASH_FULL) throw Error(DL_ERR_INTERNAL, "hash set probe sequence exceeded its capacity");
         if (err & DL_DEVERR_LOOKBACK)
             throw Error(DL_ERR_DEVICE_TIMEOUT, "a device-side wait exceeded its limit (decoupled look-back)");
         throw Error(DL_ERR_INTERNAL, "device error flag " + std::to_string(err));
@@ -155,7 +156,8 @@ const char *kernel_name(int kid) {
     static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_spine_scan", "sort_scatter_pass",
                                          "select_compact", "join_count_scan", "join_partition", "join_emit",
                                          "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build",
-                                         "sparse_diff", "host_cudaMalloc", "host_cudaFree", "host_sync"};
+                                         "sparse_diff", "hash_insert", "host_cudaMalloc", "host_cudaFree",
+                                         "host_sync"};
     return (kid >= 0 && kid < K_COUNT) ? names[kid] : "?";
 }
 

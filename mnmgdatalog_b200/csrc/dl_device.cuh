@@ -31,6 +31,7 @@ constexpr u32 kSpinLimit = 1u << 22;
 // Device error bits (ctrl->err).
 constexpr u32 DL_DEVERR_LOOKBACK = 1u;
 constexpr u32 DL_DEVERR_CAPACITY = 2u;
+constexpr u32 DL_DEVERR_HASH_FULL = 4u;
 
 // Control block resident in device memory, one per context.
 struct Ctrl {

@@ -236,6 +236,25 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
     return radix_sort(ctx, jptr, pbuf.as<u64>(), total, Codec::Raw, key_bits, hist);
 }
 
+// One join step without the sort: J in the join buffer that does not hold
+// the probe (its order follows the probe rows).
+u64 *join_unsorted(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, EmitKind kind, u64 &n_j,
+                   PhaseTimer &pt) {
+    Workspace &ws = ctx.ws;
+    pt.mark(PH_JOIN);
+    ctx.reserve(ws.offsets, std::max<u64>(n_probe, 1) * 8);
+    const u64 total = join_count(ctx, g.csr, probe, n_probe, g.bits, ws.offsets.as<u64>());
+    n_j = total;
+    ctx.run_join_total += total;
+    ctx.run_join_max = std::max(ctx.run_join_max, total);
+    DevBuf &jout = other(ws, probe);
+    ctx.reserve(jout, std::max<u64>(total, 1) * 8);
+    if (total)
+        join_emit(ctx, g.csr, probe, n_probe, g.bits, ws.offsets.as<u64>(), total, kind, jout.as<u64>(), nullptr, 0,
+                  nullptr);
+    return jout.as<u64>();
+}
+
 void finish_info(Run &r, Context &ctx, cudaEvent_t e0, cudaEvent_t e1, PhaseTimer &pt) {
     r.info.join_rows_total = (i64) ctx.run_join_total;
     r.info.join_rows_max = (i64) ctx.run_join_max;
@@ -416,6 +435,75 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     adopt_ids(ctx, r, g);
     r.words = ws.full[cur];
     ws.full[cur] = DevBuf();
+    r.n_words = nfull;
+    r.info.output_rows = r.info.output_tuples = (i64) nfull;
+    finish_info(r, ctx, ev.a, ev.b, pt);
+}
+
+// TC with the join output deduplicated by a hash set of full (dl_hashset.cu):
+// the same iterations and deltas as run_tc_impl (delta' = dedup(J) \ full is a
+// set), no per-iteration sort or merge; the result is sorted once at the end.
+static void run_tc_hash_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, bool on_device,
+                             const dl_options &opt) {
+    Workspace &ws = ctx.ws;
+    PhaseTimer pt(ctx, opt.phase_timing != 0);
+    EventPair ev;
+    DL_CUDA(cudaEventRecord(ev.a, ctx.stream));
+    pt.mark(PH_INIT);
+    const int32_t *rows = stage_input(ctx, rows_in, n, on_device);
+    Graph g;
+    u64 nfull = 0;
+    DevBuf result;
+    if (n > 0) {
+        rank_nodes(ctx, rows, n, g);
+        ctx.reserve(ws.jbuf[0], n * 8);
+        ctx.reserve(ws.jbuf[1], n * 8);
+        DL_LAUNCH(ctx, K_PREP, 0, pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
+                                                                         ws.w0.as<u64>(), ws.jbuf[0].as<u64>()));
+        u64 ne;
+        u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, n, 2 * g.bits, ne);
+        build_csr(ctx, e, ne, g);
+        u64 nd;
+        u64 *d = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * g.bits, nd);  // tc.cu:178-181
+        WordSet S;  // full (tc.cu:188-189), in ws.full[0/1]
+        wordset_reserve(ctx, S, ws.full, nd);
+        wordset_insert(ctx, S, ws.full, d, nd, nullptr);
+        u64 *delta = d;
+        u64 ndelta = nd;
+        for (int it = 0;; ++it) {  // tc.cu:216-314
+            u64 nj = 0;
+            u64 *j = join_unsorted(ctx, g, delta, ndelta, EmitKind::ZV, nj, pt);
+            pt.mark(PH_DEDUP);
+            u64 nnew = 0;
+            if (nj) {
+                wordset_reserve(ctx, S, ws.full, nj);
+                DevBuf &fb = holder(ws, delta);  // the probe is consumed: it receives the new words
+                ctx.reserve(fb, nj * 8);
+                nnew = wordset_insert(ctx, S, ws.full, j, nj, fb.as<u64>());
+                delta = fb.as<u64>();
+            }
+            ndelta = nnew;
+            r.deltas.push_back((i64) nnew);
+            r.joins.push_back((i64) nj);
+            r.fulls.push_back((i64) S.size);
+            if (nnew == 0) break;  // |full| unchanged
+            if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
+        }
+        // the program's output order: the set's words, sorted once
+        pt.mark(PH_FINAL);
+        nfull = S.size;
+        ctx.reserve(ws.jbuf[0], std::max<u64>(nfull, 1) * 8);
+        ctx.reserve(ws.jbuf[1], std::max<u64>(nfull, 1) * 8);
+        wordset_extract(ctx, S, ws.full, ws.jbuf[0].as<u64>());
+        u64 *sorted = radix_sort(ctx, ws.jbuf[0].as<u64>(), ws.jbuf[1].as<u64>(), nfull, Codec::Raw, 2 * g.bits);
+        DevBuf &hold = holder(ws, sorted);
+        result = hold;
+        hold = DevBuf();
+    }
+    DL_CUDA(cudaEventRecord(ev.b, ctx.stream));
+    pt.mark(PH_FINAL);
+    adopt_ids(ctx, r, g);
+    r.words = result;
     r.n_words = nfull;
     r.info.output_rows = r.info.output_tuples = (i64) nfull;
     finish_info(r, ctx, ev.a, ev.b, pt);
@@ -625,7 +713,10 @@ Run *run_program(Context &ctx, int program, const int32_t *rows, u64 n, bool on_
     ctx.run_join_total = ctx.run_join_max = 0;
     try {
         switch (program) {
-            case DL_PROGRAM_TC: run_tc_impl(ctx, *r, rows, n, on_device, opt); break;
+            case DL_PROGRAM_TC:
+                if (opt.dedup == DL_DEDUP_HASH) run_tc_hash_impl(ctx, *r, rows, n, on_device, opt);
+                else run_tc_impl(ctx, *r, rows, n, on_device, opt);
+                break;
             case DL_PROGRAM_SG: run_sg_impl(ctx, *r, rows, n, on_device, opt); break;
             case DL_PROGRAM_WCC: run_wcc_impl(ctx, *r, rows, n, on_device, opt); break;
             case DL_PROGRAM_SINGLE_JOIN: run_single_join_impl(ctx, *r, rows, n, on_device, opt); break;

@@ -74,6 +74,8 @@ DevBuf &holder(Workspace &ws, const u64 *p);
 DevBuf &other(Workspace &ws, const u64 *p);
 u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, EmitKind kind, u64 &n_j,
                    u64 *self_pairs, PhaseTimer &pt);
+u64 *join_unsorted(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, EmitKind kind, u64 &n_j,
+                   PhaseTimer &pt);
 u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta);
 void settle(Context &ctx, FullSet &F);
 

@@ -74,6 +74,7 @@ enum KernelId : int {
     K_MERGE,           // plain merge: 16 B per word
     K_HASH_BUILD,      // C-ABI hash table insert / value extraction
     K_SPARSE_DIFF,     // sparse set difference probes (+ run sampling)
+    K_HASH_INSERT,     // hash-set dedup: 8 B read + 32 B probe sector per word, 40 B per new word
     // host-side costs, counted with or without profiling (seconds = host wall time)
     K_HOST_MALLOC,     // cudaMalloc of a buffer that had to grow (bytes = size)
     K_HOST_FREE,       // cudaFree of a cached buffer dropped from the cache
@@ -214,6 +215,23 @@ void run_sample(Context &ctx, const u64 *run, u64 n, DevBuf &sample, u64 &ns);
 // of O(|run|). out may alias nothing in j/run; returns |out|.
 u64 sparse_diff_words(Context &ctx, const u64 *run, u64 nrun, const u64 *sample, u64 ns, const u64 *j, u64 nj,
                       u64 *out);
+
+// ---- hash set of tuple words (dl_hashset.cu) ---------------------------------
+// Open addressing over 64-bit words (empty slot = all ones), linear probing,
+// capacity a power of two, never more than 3/4 full.
+struct WordSet {
+    int cur = 0;      // which of the two buffers holds the table
+    u64 cap = 0;      // slots (power of two)
+    u64 size = 0;     // words stored
+};
+// Makes room for `incoming` more words (rehash into the other buffer when
+// size + incoming would exceed 3/4 of the capacity).
+void wordset_reserve(Context &ctx, WordSet &ws, DevBuf buf[2], u64 incoming);
+// Inserts n words; the ones not present before go to `fresh` (if not null),
+// in no particular order. Returns how many were new.
+u64 wordset_insert(Context &ctx, WordSet &ws, DevBuf buf[2], const u64 *in, u64 n, u64 *fresh);
+// Copies the stored words (unsorted) to out (size words); returns size.
+u64 wordset_extract(Context &ctx, const WordSet &ws, DevBuf buf[2], u64 *out);
 
 // ---- joins (dl_join.cu) --------------------------------------------------------
 struct Csr {            // relation grouped by dense key index

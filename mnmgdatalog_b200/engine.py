@@ -149,7 +149,8 @@ class Engine:
 
     # ---- programs ----------------------------------------------------------
     def run(self, program: str, edges, *, wcc_stop: str = "reference", max_iterations: int = 0,
-            phase_timing: bool = False, output: str = "host", labels: bool = False, out=None) -> RunResult:
+            phase_timing: bool = False, output: str = "host", labels: bool = False, out=None,
+            dedup: str = "auto") -> RunResult:
         """Run one program. `edges` is an (n, 2) int32 host array or a CUDA
         tensor (then the input stays on the device). `output` is "host"
         (numpy), "device" (torch tensor) or "none"; `out` optionally supplies
@@ -161,6 +162,7 @@ class Engine:
         opts.wcc_stop = {"reference": capi.WCC_STOP_REFERENCE, "fixpoint": capi.WCC_STOP_FIXPOINT}[wcc_stop]
         opts.max_iterations = max_iterations
         opts.phase_timing = 1 if phase_timing else 0
+        opts.dedup = {"auto": capi.DEDUP_AUTO, "sort": capi.DEDUP_SORT, "hash": capi.DEDUP_HASH}[dedup]
         keep = None
         if isinstance(edges, torch.Tensor) and edges.is_cuda:
             keep = _check_rel(edges) if edges.numel() else edges

@@ -34,6 +34,7 @@ CLASSES = [
     (r"merge_kernel", "merge"),
     (r"sparse_mark_kernel|sample_kernel", "sparse_diff"),
     (r"hash_insert_kernel|extract_values_kernel", "hash_build"),
+    (r"wordset_insert_kernel|wordset_rehash_kernel", "hash_insert"),
 ]
 
 

@@ -111,3 +111,39 @@ def test_phase_timing(engine):
     assert r.seconds > 0 and set(r.phases) == {"initialization", "join", "deduplication", "merge",
                                                "finalization"}
     assert sum(r.phases.values()) > 0
+
+
+TC_FILES = [f for f, e in EXP["inputs"].items() if "tc" in e]
+
+
+@pytest.mark.parametrize("fname", TC_FILES)
+@pytest.mark.parametrize("dedup", ["sort", "hash"])
+def test_tc_dedup_modes(engine, fname, dedup):
+    """Both ways of removing known tuples give the reference's rows, iteration
+    count and per-iteration deltas."""
+    e = load_input(fname)
+    rec = EXP["inputs"][fname]["tc"]
+    r = engine.tc(e, dedup=dedup)
+    assert r.iterations == rec["iterations"]
+    assert r.deltas.tolist() == rec["deltas"]
+    assert sha_rows(r.rows) == rec["rows_sha256"]
+
+
+@pytest.mark.parametrize("dedup", ["sort", "hash"])
+def test_tc_dedup_modes_edge_cases(engine, dedup):
+    for name, e in _edge_cases():
+        got = engine.tc(e, dedup=dedup)
+        want = cpu.tc(e)
+        assert np.array_equal(got.rows, want.rows), name
+        assert got.deltas.tolist() == list(want.deltas), name
+
+
+def test_tc_dedup_modes_agree_at_scale(engine):
+    """A closure of ~3e7 tuples (hash-set growth and rehash on the way)."""
+    from mnmgdatalog_b200 import graphs
+    import torch
+    e = torch.from_numpy(graphs.chung_lu(n=40_000, m=132_500, seed=0)).cuda()
+    a = engine.tc(e, dedup="sort", output="device")
+    b = engine.tc(e, dedup="hash", output="device")
+    assert a.iterations == b.iterations and a.deltas.tolist() == b.deltas.tolist()
+    assert torch.equal(a.rows, b.rows)
