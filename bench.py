@@ -351,10 +351,14 @@ def measure_batched(eng, dev, args) -> dict:
     time, inputs resident in HBM for both, outputs left on the device."""
     import torch
 
-    from mnmgdatalog_b200 import graphs
+    from mnmgdatalog_b200 import autotune, graphs
     work = graphs.batched_workload(count=args.batch_instances, seed=0)
     groups = {p: [torch.from_numpy(e).to(dev) for q, e in work if q == p] for p in ("tc", "wcc")}
     torch.cuda.synchronize(dev)
+    # knobs picked by the autotuner on a sample (every 8th TC instance; its
+    # deltas must not change), then used for the whole batch and the plain runs
+    before = eng.tuning()
+    tuned = autotune.autotune_batch(eng, "tc", groups["tc"][::8], repeats=1, log=lambda *_: None)["tuning"]
     for _ in range(max(1, min(args.warmup, 2))):
         for p, g in groups.items():
             eng.run_batch(p, g, output="none")
@@ -372,6 +376,7 @@ def measure_batched(eng, dev, args) -> dict:
     same = all(a.iterations == b.iterations and a.output_tuples == b.output_tuples
                and a.deltas.tolist() == b.deltas.tolist()
                for p in groups for a, b in zip(batched[p], plain[p]))
+    eng.set_tuning(before)
     n = sum(len(g) for g in groups.values())
     tuples = sum(r.output_tuples for p in ("tc",) for r in plain[p])
     return {"workload": f"{n} instances: {len(groups['tc'])} TC on DAGs + {len(groups['wcc'])} WCC on Chung-Lu "
@@ -379,7 +384,7 @@ def measure_batched(eng, dev, args) -> dict:
             "edges_total": int(sum(len(e) for _, e in work)), "tc_tuples": int(tuples),
             "queries_per_s": n / t_batch, "plain_queries_per_s": n / t_plain,
             "speedup_vs_plain": t_plain / t_batch, "seconds": t_batch, "plain_seconds": t_plain,
-            "reps": reps, "identical_to_plain": bool(same),
+            "reps": reps, "identical_to_plain": bool(same), "tuning": tuned,
             "timer": "host wall clock around dl_run_batch per program (synchronized), inputs in HBM",
             "form": "union fixpoint per program (one launch sequence per iteration for all instances)"}
 

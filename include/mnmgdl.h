@@ -120,6 +120,21 @@ DL_API dl_status dl_context_create(int32_t device, void *stream, dl_context **ou
 DL_API dl_status dl_context_destroy(dl_context *ctx);
 DL_API dl_status dl_context_synchronize(dl_context *ctx);
 DL_API dl_status dl_free(dl_context *ctx, void *device_ptr);
+
+/* Engine knobs of a context (no counterpart in the reference; set by the
+ * autotuner, mnmgdatalog_b200/autotune.py). Results never depend on them. */
+typedef struct dl_tuning {
+    int32_t sort_algorithm;       /* 1 = three-kernel LSD radix pass (default), 0 = onesweep */
+    int32_t sort_ranking;         /* 1 = shared-memory peer masks (default), 0 = warp ballots */
+    int32_t sort_keys_per_thread; /* onesweep tile: 16 (default) or 12 */
+    int32_t dense_ratio;          /* TC/SG: one fused rewrite of full when |J| * ratio >= |large run| (1..64, default 4) */
+    int32_t small_ratio;          /* TC/SG: small run folded into the large one at |small| * ratio >= |large| (1..64, default 4) */
+    int32_t reserved0;
+    double hash_load_factor;      /* dl_build_hash_table's default load factor (0 < lf < 1, default 0.5) */
+    int32_t reserved[4];
+} dl_tuning;
+DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out);
+DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *tuning);
 /* Copy `bytes` between any two host/device buffers on the context's stream
  * and wait for it (cudaMemcpyDefault). */
 DL_API dl_status dl_memcpy(dl_context *ctx, void *dst, const void *src, int64_t bytes);

@@ -26,6 +26,7 @@ DEDUP_AUTO, DEDUP_SORT, DEDUP_HASH = 0, 1, 2
 EXPORTS = (
     "dl_status_string", "dl_last_error", "dl_version",
     "dl_context_create", "dl_context_destroy", "dl_context_synchronize", "dl_free", "dl_memcpy",
+    "dl_context_get_tuning", "dl_context_set_tuning",
     "dl_sort_unique", "dl_sort", "dl_set_difference", "dl_merge", "dl_diff_merge",
     "dl_unique_by_key_min", "dl_remove_self_pairs",
     "dl_build_hash_table", "dl_hash_table_info", "dl_hash_table_destroy", "dl_join", "dl_join_sorted",
@@ -60,6 +61,12 @@ class dl_run_info(C.Structure):
                 ("seconds_finalize", C.c_double), ("join_rows_total", C.c_int64), ("join_rows_max", C.c_int64)]
 
 
+class dl_tuning(C.Structure):
+    _fields_ = [("sort_algorithm", C.c_int32), ("sort_ranking", C.c_int32), ("sort_keys_per_thread", C.c_int32),
+                ("dense_ratio", C.c_int32), ("small_ratio", C.c_int32), ("reserved0", C.c_int32),
+                ("hash_load_factor", C.c_double), ("reserved", C.c_int32 * 4)]
+
+
 class dl_kernel_stat(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("timed_launches", C.c_int64),
                 ("seconds", C.c_double), ("bytes", C.c_double)]
@@ -87,6 +94,8 @@ def lib():
         "dl_context_synchronize": ([vp], C.c_int),
         "dl_free": ([vp, vp], C.c_int),
         "dl_memcpy": ([vp, vp, vp, i64], C.c_int),
+        "dl_context_get_tuning": ([vp, C.POINTER(dl_tuning)], C.c_int),
+        "dl_context_set_tuning": ([vp, C.POINTER(dl_tuning)], C.c_int),
         "dl_sort_unique": ([vp, vp, i64, pi64], C.c_int),
         "dl_sort": ([vp, vp, i64], C.c_int),
         "dl_set_difference": ([vp, vp, i64, vp, i64, vp, pi64], C.c_int),

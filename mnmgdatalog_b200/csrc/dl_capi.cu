@@ -601,6 +601,37 @@ DL_API dl_status dl_run_batch(dl_context *ctx, int32_t program, const int32_t *c
     return DL_OK;
 }
 
+DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out) {
+    DL_REQUIRE(ctx && out, "invalid argument");
+    const dl::Tuning &t = ctx->c.tune;
+    std::memset(out, 0, sizeof(*out));
+    out->sort_algorithm = t.sort_algo;
+    out->sort_ranking = t.rank;
+    out->sort_keys_per_thread = t.sort_kpt;
+    out->dense_ratio = (int32_t) t.dense_ratio;
+    out->small_ratio = (int32_t) t.small_ratio;
+    out->hash_load_factor = t.hash_load;
+    return DL_OK;
+}
+
+DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
+    DL_REQUIRE(ctx && t, "invalid argument");
+    DL_REQUIRE(t->sort_algorithm == 0 || t->sort_algorithm == 1, "sort_algorithm must be 0 or 1");
+    DL_REQUIRE(t->sort_ranking == 0 || t->sort_ranking == 1, "sort_ranking must be 0 or 1");
+    DL_REQUIRE(t->sort_keys_per_thread == 12 || t->sort_keys_per_thread == 16, "sort_keys_per_thread must be 12 or 16");
+    DL_REQUIRE(t->dense_ratio >= 1 && t->dense_ratio <= 64, "dense_ratio must be in 1..64");
+    DL_REQUIRE(t->small_ratio >= 1 && t->small_ratio <= 64, "small_ratio must be in 1..64");
+    DL_REQUIRE(t->hash_load_factor > 0.0 && t->hash_load_factor < 1.0, "hash_load_factor must be in (0, 1)");
+    dl::Tuning &o = ctx->c.tune;
+    o.sort_algo = t->sort_algorithm;
+    o.rank = t->sort_ranking;
+    o.sort_kpt = t->sort_keys_per_thread;
+    o.dense_ratio = (u64) t->dense_ratio;
+    o.small_ratio = (u64) t->small_ratio;
+    o.hash_load = t->hash_load_factor;
+    return DL_OK;
+}
+
 DL_API dl_status dl_profile_enable(dl_context *ctx, int32_t enabled) {
     DL_REQUIRE(ctx, "ctx is NULL");
     return guarded([&] {

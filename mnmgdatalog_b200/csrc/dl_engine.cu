@@ -222,7 +222,7 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
     ctx.reserve(jout, std::max<u64>(total, 1) * 8);
     if (total == 0) return jout.as<u64>();
     const int key_bits = 2 * g.bits;
-    const bool fuse_hist = radix_wants_histogram() && !g.nwin;
+    const bool fuse_hist = radix_wants_histogram(ctx) && !g.nwin;
     const int ndig = fuse_hist ? (key_bits + 7) / 8 : 0;
     u64 *hist = fuse_hist ? radix_hist_buffer(ctx) : nullptr;
     if (fuse_hist) radix_hist_clear(ctx);
@@ -306,8 +306,8 @@ void adopt_ids(Context &ctx, Run &r, const Graph &g) {
 // streaming step ~13 ps per word of (large run + J), so probing wins while
 // |J| is below ~1/3 of the large run; the small run is folded into the large
 // one only once it reaches 1/4 of it (otherwise at the end).
-constexpr u64 kDenseRatio = 4;   // J is dense when |J| * 4 >= |large run|
-constexpr u64 kSmallRatio = 4;   // merge when |small run| * 4 >= |large run|
+// The thresholds are per-context tuning (Tuning::dense_ratio, small_ratio;
+// defaults 4 and 4).
 
 // Sorted J (in one of ws.jbuf) -> delta (returned, in one of ws.jbuf);
 // updates the full relation. Returns |delta| in n_delta.
@@ -315,7 +315,7 @@ u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta) {
     Workspace &ws = ctx.ws;
     n_delta = 0;
     if (nj == 0) return j;
-    const bool dense = nj * kDenseRatio >= F.nbig;
+    const bool dense = nj * ctx.tune.dense_ratio >= F.nbig;
     DevBuf &d1buf = other(ws, j);
     if (F.nsmall == 0 && dense) {
         // fused: delta and the new large run in one pass
@@ -353,7 +353,7 @@ u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta) {
         F.nsmall += n;
     }
     n_delta = n;
-    if (F.nsmall && F.nsmall * kSmallRatio >= F.nbig) {
+    if (F.nsmall && F.nsmall * ctx.tune.small_ratio >= F.nbig) {
         ctx.reserve(ws.full[1 - F.cur], (F.nbig + F.nsmall) * 8);
         merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.small[F.scur].as<u64>(), F.nsmall,
                     ws.full[1 - F.cur].as<u64>(), Codec::Raw);

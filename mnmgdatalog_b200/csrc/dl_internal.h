@@ -104,8 +104,22 @@ struct Workspace {
     DevBuf wcc_label, wcc_flag, wcc_next;
 };
 
+// Engine knobs the autotuner sets per context (mnmgdatalog_b200/autotune.py);
+// the defaults are the measured best on B200. DL_SORT_ALGO, DL_SORT_RANK and
+// DL_SORT_KPT override the sort defaults.
+struct Tuning {
+    int sort_algo = 1;          // 1 = three-kernel LSD pass, 0 = onesweep
+    int rank = 1;               // 1 = shared-memory peer masks, 0 = warp ballots
+    int sort_kpt = 16;          // onesweep keys per thread: 12 or 16
+    u64 dense_ratio = 4;        // fused full rewrite when |J| * dense_ratio >= |large run|
+    u64 small_ratio = 4;        // small run folded when |small| * small_ratio >= |large run|
+    double hash_load = 0.5;     // default load factor of dl_build_hash_table
+};
+Tuning default_tuning();
+
 struct Context {
     int device = 0;
+    Tuning tune = default_tuning();
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int sm_count = 148;
@@ -186,7 +200,7 @@ u64 *radix_hist_buffer(Context &ctx);
 void radix_hist_clear(Context &ctx);
 // True when radix_sort benefits from a producer-accumulated histogram
 // (the onesweep variant); the three-kernel variant counts per chunk itself.
-bool radix_wants_histogram();
+bool radix_wants_histogram(const Context &ctx);
 
 // ---- compaction / scan (dl_scan.cu) ------------------------------------------
 // out[i] = in[i] for the first of each run of equal words; returns count.

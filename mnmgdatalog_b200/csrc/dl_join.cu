@@ -90,7 +90,7 @@ __global__ void extract_values_kernel(const u64 *__restrict__ sorted, u64 n, u32
 }  // namespace
 
 HashTable *hash_table_build(Context &ctx, const u64 *rel, u64 n, double load_factor) {
-    if (!(load_factor > 0.0 && load_factor < 1.0)) load_factor = 0.5;
+    if (!(load_factor > 0.0 && load_factor < 1.0)) load_factor = ctx.tune.hash_load;
     if (n > 0xFFFFFFFFull) throw Error(DL_ERR_OVERFLOW, "hash table relation exceeds 2^32 rows");
     auto *ht = new HashTable();
     ht->rows = n;

@@ -186,30 +186,28 @@ onesweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int sh
     }
 }
 
-// Ranking variant: DL_SORT_RANK=ballot|atomic (default atomic), read once.
-int rank_mode() {
-    static int mode = -1;
-    if (mode < 0) {
+}  // namespace
+
+Tuning default_tuning() {
+    static const Tuning t = [] {
+        Tuning d;
         const char *e = getenv("DL_SORT_RANK");
-        mode = (e && std::string(e) == "ballot") ? RANK_BALLOT : RANK_ATOMIC;
-    }
-    return mode;
+        if (e && std::string(e) == "ballot") d.rank = RANK_BALLOT;
+        e = getenv("DL_SORT_KPT");
+        if (e && std::string(e) == "12") d.sort_kpt = 12;
+        e = getenv("DL_SORT_ALGO");
+        if (e && std::string(e) == "onesweep") d.sort_algo = 0;
+        return d;
+    }();
+    return t;
 }
 
-// Keys per thread of a onesweep tile: DL_SORT_KPT=12|16 (default 16), read once.
-int sort_kpt() {
-    static int k = -1;
-    if (k < 0) {
-        const char *e = getenv("DL_SORT_KPT");
-        k = (e && std::string(e) == "12") ? 12 : 16;
-    }
-    return k;
-}
+namespace {
 
 template <bool ENC, bool DEC, int KPT, int MINB>
 void launch_onesweep_k(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, const u64 *bucket, u64 *lb, u32 *ctr) {
-    auto kern = rank_mode() == RANK_BALLOT ? onesweep_kernel<ENC, DEC, RANK_BALLOT, KPT, MINB>
-                                           : onesweep_kernel<ENC, DEC, RANK_ATOMIC, KPT, MINB>;
+    auto kern = ctx.tune.rank == RANK_BALLOT ? onesweep_kernel<ENC, DEC, RANK_BALLOT, KPT, MINB>
+                                             : onesweep_kernel<ENC, DEC, RANK_ATOMIC, KPT, MINB>;
     const int smem = (int) sizeof(SortSmem<KPT>);
     DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const u64 tile = (u64) SORT_THREADS * KPT;
@@ -219,12 +217,12 @@ void launch_onesweep_k(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, 
                                                                           ctx.next_epoch(), &ctx.ctrl->err));
 }
 
-u64 sort_tile_keys() { return (u64) SORT_THREADS * sort_kpt(); }
+u64 sort_tile_keys(const Context &ctx) { return (u64) SORT_THREADS * ctx.tune.sort_kpt; }
 
 template <bool ENC, bool DEC>
 void launch_onesweep(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, const u64 *bucket, u64 *lb,
                      u32 *ctr) {
-    if (sort_kpt() == 12) launch_onesweep_k<ENC, DEC, 12, 3>(ctx, in, out, n, shift, bucket, lb, ctr);
+    if (ctx.tune.sort_kpt == 12) launch_onesweep_k<ENC, DEC, 12, 3>(ctx, in, out, n, shift, bucket, lb, ctr);
     else launch_onesweep_k<ENC, DEC, 16, 2>(ctx, in, out, n, shift, bucket, lb, ctr);
 }
 
@@ -295,7 +293,7 @@ struct WordValue {
     __device__ __forceinline__ u64 operator()(u64 i) const { return v[i]; }
 };
 
-template <bool ENC, bool DEC>
+template <bool ENC, bool DEC, int RANK>
 __global__ void __launch_bounds__(DS_THREADS, 2)
 radix_downsweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n, int shift, u64 chunk, u32 G,
                        const u64 *__restrict__ offsets, int use_tma, u32 *err) {
@@ -365,16 +363,27 @@ radix_downsweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n,
 #pragma unroll
         for (int i = 0; i < DS_KPT; ++i) {
             const u32 d = (u32) (k[i] >> shift) & 255u;
-            atomicOr(&s.match[w][d], 1u << lane);
-            __syncwarp();
-            const u32 peers = *reinterpret_cast<volatile u32 *>(&s.match[w][d]);
-            __syncwarp();
+            u32 peers;
+            if (RANK == RANK_BALLOT) {  // lanes with the same digit: one ballot per digit bit
+                peers = 0xffffffffu;
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    const u32 bit = (d >> b) & 1u;
+                    const u32 bal = __ballot_sync(0xffffffffu, bit);
+                    peers &= bit ? bal : ~bal;
+                }
+            } else {
+                atomicOr(&s.match[w][d], 1u << lane);
+                __syncwarp();
+                peers = *reinterpret_cast<volatile u32 *>(&s.match[w][d]);
+                __syncwarp();
+            }
             const u32 leader = __ffs(peers) - 1;
             u32 prev = 0;
             if (lane == leader) {
                 prev = s.warp_cnt[w][d];
                 s.warp_cnt[w][d] = prev + __popc(peers);
-                s.match[w][d] = 0;
+                if (RANK == RANK_ATOMIC) s.match[w][d] = 0;
             }
             __syncwarp();
             prev = __shfl_sync(0xffffffffu, prev, leader);
@@ -420,15 +429,7 @@ radix_downsweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n,
     }
 }
 
-// Sort algorithm: DL_SORT_ALGO=onesweep|lsd3 (default lsd3), read once.
-bool use_lsd3() {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = getenv("DL_SORT_ALGO");
-        v = (e && std::string(e) == "onesweep") ? 0 : 1;
-    }
-    return v == 1;
-}
+bool use_lsd3(const Context &ctx) { return ctx.tune.sort_algo == 1; }
 
 template <bool ENC, bool DEC>
 void lsd3_pass(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, u32 G, u64 chunk, u64 *hist, u64 *offs) {
@@ -442,7 +443,8 @@ void lsd3_pass(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, u32 G, u
     DL_LAUNCH(ctx, K_SORT_BUCKET, 16.0 * m,
               scan_kernel<WordValue><<<(unsigned) tiles, SCAN_THREADS, 0, ctx.stream>>>(
                   WordValue{hist}, m, offs, lb, ctr, ctx.next_epoch(), &ctx.ctrl->err, &ctx.ctrl->scalar[12]));
-    auto kern = radix_downsweep_kernel<ENC, DEC>;
+    auto kern = ctx.tune.rank == RANK_BALLOT ? radix_downsweep_kernel<ENC, DEC, RANK_BALLOT>
+                                             : radix_downsweep_kernel<ENC, DEC, RANK_ATOMIC>;
     const int smem = (int) sizeof(DsSmem);
     DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int use_tma = ((reinterpret_cast<uintptr_t>(in) & 15u) == 0) ? 1 : 0;
@@ -465,7 +467,7 @@ void lsd3_grid(Context &ctx, u64 n, u64 &G, u64 &chunk) {
 
 u64 *radix_sort_windows(Context &ctx, u64 *a, u64 *b, u64 n, const int *shifts, int nwin) {
     if (n <= 1 || nwin <= 0) return a;
-    if (!use_lsd3()) return radix_sort(ctx, a, b, n, Codec::Raw, shifts[nwin - 1] + 8);
+    if (!use_lsd3(ctx)) return radix_sort(ctx, a, b, n, Codec::Raw, shifts[nwin - 1] + 8);
     u64 G, chunk;
     lsd3_grid(ctx, n, G, chunk);
     u64 *ph = ctx.radix_part.as<u64>();
@@ -516,7 +518,7 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
     int nd = 0;
     DL_CUDA(cudaMemsetAsync(ctr, 0, 17 * sizeof(u32), ctx.stream));
     const int ndig = (known_bits > 0 && !ent) ? (known_bits + 7) / 8 : 8;
-    const bool lsd3 = use_lsd3();
+    const bool lsd3 = use_lsd3(ctx);
     if (known_bits > 0 && !ent) {
         for (int d = 0; d < ndig; ++d) digits[nd++] = d;
     }
@@ -563,7 +565,7 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
         }
         return const_cast<u64 *>(src);
     }
-    const u64 tiles = (n + sort_tile_keys() - 1) / sort_tile_keys();
+    const u64 tiles = (n + sort_tile_keys(ctx) - 1) / sort_tile_keys(ctx);
     u64 *lb = ctx.lookback_words(tiles * RADIX);
     for (int p = 0; p < nd; ++p) {
         const bool enc = ent && p == 0, dec = ent && p == nd - 1;
@@ -580,6 +582,6 @@ u64 *radix_sort(Context &ctx, u64 *a, u64 *b, u64 n, Codec codec, int known_bits
     return const_cast<u64 *>(src);
 }
 
-bool radix_wants_histogram() { return !use_lsd3(); }
+bool radix_wants_histogram(const Context &ctx) { return !use_lsd3(ctx); }
 
 }  // namespace dl

@@ -343,7 +343,7 @@ void full_insert_new(SessionImpl &s, const u64 *w, u64 n) {
     merge_words(ctx, ws.small[F.scur].as<u64>(), F.nsmall, w, n, ws.small[1 - F.scur].as<u64>(), Codec::Raw);
     F.scur = 1 - F.scur;
     F.nsmall += n;
-    if (F.nsmall * 4 >= F.nbig) {
+    if (F.nsmall * ctx.tune.small_ratio >= F.nbig) {
         ctx.reserve(ws.full[1 - F.cur], (F.nbig + F.nsmall) * 8);
         merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.small[F.scur].as<u64>(), F.nsmall,
                     ws.full[1 - F.cur].as<u64>(), Codec::Raw);
@@ -707,6 +707,7 @@ SessionImpl *session_create(Context &parent, int program, const dl_options &opt,
     c.stream = parent.stream;
     c.sm_count = parent.sm_count;
     c.prof_on = parent.prof_on;
+    c.tune = parent.tune;
     void *p = nullptr;
     DL_CUDA(cudaMalloc(&p, sizeof(Ctrl)));
     c.ctrl = (Ctrl *) p;

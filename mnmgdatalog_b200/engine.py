@@ -134,6 +134,32 @@ class Engine:
     def synchronize(self):
         check(lib().dl_context_synchronize(self.ctx))
 
+    TUNING_FIELDS = ("sort_algorithm", "sort_ranking", "sort_keys_per_thread", "dense_ratio", "small_ratio",
+                     "hash_load_factor")
+
+    def tuning(self) -> dict:
+        """The context's engine knobs (dl_tuning)."""
+        t = capi.dl_tuning()
+        check(lib().dl_context_get_tuning(self.ctx, C.byref(t)))
+        return {f: getattr(t, f) for f in self.TUNING_FIELDS}
+
+    def set_tuning(self, tuning: dict | None = None, **kw) -> None:
+        """Sets engine knobs (unspecified ones keep their value); results do
+        not depend on them. `tuning` may be a dict or a JSON file path."""
+        if isinstance(tuning, str):
+            import json
+            with open(tuning) as f:
+                tuning = json.load(f)
+            tuning = tuning.get("tuning", tuning)
+        cur = self.tuning()
+        cur.update({k: v for k, v in (tuning or {}).items() if k in self.TUNING_FIELDS})
+        cur.update({k: v for k, v in kw.items() if k in self.TUNING_FIELDS})
+        unknown = set(kw) - set(self.TUNING_FIELDS)
+        if unknown:
+            raise DatalogError(1, f"unknown tuning fields {sorted(unknown)}")
+        t = capi.dl_tuning(**cur)
+        check(lib().dl_context_set_tuning(self.ctx, C.byref(t)))
+
     def profile(self, enabled: bool = True) -> None:
         """Reset the live kernel profile; enabled=True times every launch."""
         check(lib().dl_profile_enable(self.ctx, 1 if enabled else 0))
