@@ -127,7 +127,7 @@ class Server:
 
     def __init__(self, engine=None, *, budget_bytes: int = 150 * 10**9, wcc_stop: str = "reference",
                  max_active: int = 0, backend=None, clock=time.perf_counter, keep_results: bool = True,
-                 concurrent: bool = False, output: str = "host", pinned: bool = False):
+                 concurrent: bool = False, output: str = "host", pinned: bool = False, tuning: dict | None = None):
         self.budget = int(budget_bytes)
         self.output = output  # where result rows go: "host" (delivered), "device" or "none"
         self.pool = PinnedPool() if (pinned and output == "host") else None
@@ -144,6 +144,8 @@ class Server:
                 backend = {}
                 for p in PROGRAMS:
                     e = Engine(engine.device)
+                    if tuning:
+                        e.set_tuning(tuning)
                     self._engines.append(e)
                     backend[p] = (lambda p=p, e=e: e.session(p, wcc_stop=wcc_stop))
             else:
@@ -161,6 +163,14 @@ class Server:
         self._t0 = 0.0
         import threading
         self._pool_lock = threading.Lock()
+
+    def reset_stats(self) -> None:
+        """Forgets the counters of previous serve() calls (sessions stay)."""
+        self.finished = []
+        self.steps = 0
+        self.max_active_seen = 0
+        self.peak_bytes = 0
+        self.budget_waits = 0
 
     def close(self):
         for s in self.sessions.values():
@@ -267,6 +277,7 @@ class Server:
 
     def serve(self, requests: list[Request], *, idle_sleep: float = 0.0002) -> ServeStats:
         """Runs the request stream (arrival times relative to the start)."""
+        self.reset_stats()
         if self.concurrent:
             return self._serve_threads(requests)
         pending = sorted(requests, key=lambda r: r.arrival)
