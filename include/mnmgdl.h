@@ -129,7 +129,7 @@ typedef struct dl_tuning {
     int32_t sort_keys_per_thread; /* onesweep tile: 16 (default) or 12 */
     int32_t dense_ratio;          /* TC/SG: one fused rewrite of full when |J| * ratio >= |large run| (1..64, default 4) */
     int32_t small_ratio;          /* TC/SG: small run folded into the large one at |small| * ratio >= |large| (1..64, default 4) */
-    int32_t reserved0;
+    int32_t sort_input_tma;       /* three-kernel pass input: 1 = TMA double buffer (default), 0 = direct loads */
     double hash_load_factor;      /* dl_build_hash_table's default load factor (0 < lf < 1, default 0.5) */
     int32_t reserved[4];
 } dl_tuning;

@@ -105,12 +105,13 @@ struct Workspace {
 };
 
 // Engine knobs the autotuner sets per context (mnmgdatalog_b200/autotune.py);
-// the defaults are the measured best on B200. DL_SORT_ALGO, DL_SORT_RANK and
-// DL_SORT_KPT override the sort defaults.
+// the defaults are the measured best on B200. DL_SORT_ALGO, DL_SORT_RANK,
+// DL_SORT_KPT and DL_SORT_TMA override the sort defaults.
 struct Tuning {
     int sort_algo = 1;          // 1 = three-kernel LSD pass, 0 = onesweep
     int rank = 1;               // 1 = shared-memory peer masks, 0 = warp ballots
     int sort_kpt = 16;          // onesweep keys per thread: 12 or 16
+    int sort_tma = 1;           // three-kernel pass input: 1 = TMA double buffer, 0 = direct loads
     u64 dense_ratio = 4;        // fused full rewrite when |J| * dense_ratio >= |large run|
     u64 small_ratio = 4;        // small run folded when |small| * small_ratio >= |large run|
     double hash_load = 0.5;     // default load factor of dl_build_hash_table

@@ -197,6 +197,8 @@ Tuning default_tuning() {
         if (e && std::string(e) == "12") d.sort_kpt = 12;
         e = getenv("DL_SORT_ALGO");
         if (e && std::string(e) == "onesweep") d.sort_algo = 0;
+        e = getenv("DL_SORT_TMA");
+        if (e && std::string(e) == "0") d.sort_tma = 0;
         return d;
     }();
     return t;
@@ -245,7 +247,6 @@ struct DsSmem {
     u32 match[DS_WARPS][RADIX];
     u64 run_off[RADIX];
     u64 gbase[RADIX];
-    u32 tile_start[RADIX];
     u32 scratch[DS_WARPS + 1];
     u64 bar[2];
 };
@@ -405,7 +406,9 @@ radix_downsweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n,
         u32 total;
         const u32 start = block_exclusive_sum<DS_WARPS>(tid < RADIX ? cnt_all : 0u, s.scratch, &total);
         if (tid < RADIX) {
-            s.tile_start[tid] = start;
+            // warp_cnt[w][d] becomes the tile position of warp w's first key of digit d
+#pragma unroll
+            for (int ww = 0; ww < DS_WARPS; ++ww) s.warp_cnt[ww][tid] += start;
             s.gbase[tid] = s.run_off[tid] - start;
             s.run_off[tid] += cnt_valid;
         }
@@ -413,7 +416,7 @@ radix_downsweep_kernel(const u64 *__restrict__ in, u64 *__restrict__ out, u64 n,
 #pragma unroll
         for (int i = 0; i < DS_KPT; ++i) {
             const u32 d = (u32) (k[i] >> shift) & 255u;
-            buf[s.tile_start[d] + s.warp_cnt[w][d] + rank[i]] = k[i];
+            buf[s.warp_cnt[w][d] + rank[i]] = k[i];
         }
         __syncthreads();
         if (tid < RADIX)
@@ -447,7 +450,7 @@ void lsd3_pass(Context &ctx, const u64 *in, u64 *out, u64 n, int shift, u32 G, u
                                              : radix_downsweep_kernel<ENC, DEC, RANK_ATOMIC>;
     const int smem = (int) sizeof(DsSmem);
     DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const int use_tma = ((reinterpret_cast<uintptr_t>(in) & 15u) == 0) ? 1 : 0;
+    const int use_tma = (ctx.tune.sort_tma && (reinterpret_cast<uintptr_t>(in) & 15u) == 0) ? 1 : 0;
     DL_LAUNCH(ctx, K_SORT_PASS, 16.0 * n,
               kern<<<G, DS_THREADS, smem, ctx.stream>>>(in, out, n, shift, chunk, G, offs, use_tma, &ctx.ctrl->err));
 }

@@ -134,8 +134,8 @@ class Engine:
     def synchronize(self):
         check(lib().dl_context_synchronize(self.ctx))
 
-    TUNING_FIELDS = ("sort_algorithm", "sort_ranking", "sort_keys_per_thread", "dense_ratio", "small_ratio",
-                     "hash_load_factor")
+    TUNING_FIELDS = ("sort_algorithm", "sort_ranking", "sort_keys_per_thread", "sort_input_tma", "dense_ratio",
+                     "small_ratio", "hash_load_factor")
 
     def tuning(self) -> dict:
         """The context's engine knobs (dl_tuning)."""
