@@ -294,13 +294,16 @@ void adopt_ids(Context &ctx, Run &r, const Graph &g) {
     r.info.nodes = g.n_ids;
 }
 
-// The full relation of TC/SG as two disjoint sorted duplicate-free runs: a
-// large one (ws.full[cur]) and a small one (ws.small[scur]). The reference
-// keeps one sorted array and re-merges it with every delta (tc.cu:260-286),
-// which costs O(|full|) per iteration even when the delta is tiny; here a
-// sparse join output is checked against the large run by binary probes and
-// only the small run is rewritten, and the small run is merged into the large
-// one when it reaches 1/4 of it. The iteration's delta is the same set.
+// The full relation of TC/SG as disjoint sorted duplicate-free runs: a large
+// one (ws.full[cur]), a small one (ws.small[scur]) and, for plain runs, a
+// tiny one (ws.tiny[tcur]). The reference keeps one sorted array and
+// re-merges it with every delta (tc.cu:260-286), which costs O(|full|) per
+// iteration even when the delta is tiny; here a sparse join output is checked
+// against the large run by binary probes and only the small run is
+// rewritten, and the small run is merged into the large one when it reaches
+// 1/4 of it. Late iterations whose deltas are small against the small run
+// probe it as well and rewrite only the tiny run, which is folded into the
+// small run at 1/4 of it. The iteration's delta is the same set.
 
 // Measured on B200: a binary probe costs ~50 ps per J word, the fused
 // streaming step ~13 ps per word of (large run + J), so probing wins while
@@ -343,14 +346,38 @@ u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta) {
                                 d1buf.as<u64>());
     }
     if (nd1 == 0) return j;
+    DevBuf &jb = holder(ws, j);  // J is consumed
+    if (F.three && F.nsmall && nd1 * ctx.tune.dense_ratio < F.nsmall) {
+        // delta'' = delta' \ small run by probes; delta = delta'' \ tiny run,
+        // tiny run' = tiny run u delta
+        if (!F.ssample_ok) {
+            run_sample(ctx, ws.small[F.scur].as<u64>(), F.nsmall, ws.sample_small, F.nss);
+            F.ssample_ok = true;
+        }
+        ctx.reserve(jb, std::max<u64>(nd1, 1) * 8);
+        const u64 nd2 = sparse_diff_words(ctx, ws.small[F.scur].as<u64>(), F.nsmall, ws.sample_small.as<u64>(),
+                                          F.nss, d1buf.as<u64>(), nd1, jb.as<u64>());
+        if (nd2 == 0) return jb.as<u64>();
+        ctx.reserve(ws.tiny[1 - F.tcur], (F.ntiny + nd2) * 8);
+        const u64 n = diff_merge_words(ctx, ws.tiny[F.tcur].as<u64>(), F.ntiny, jb.as<u64>(), nd2,
+                                       ws.tiny[1 - F.tcur].as<u64>(), d1buf.as<u64>(), Codec::Raw);
+        if (n) {
+            F.tcur = 1 - F.tcur;
+            F.ntiny += n;
+        }
+        n_delta = n;
+        if (F.ntiny * ctx.tune.small_ratio >= F.nsmall) fold_tiny(ctx, F);
+        return d1buf.as<u64>();
+    }
+    fold_tiny(ctx, F);  // the small run below is the whole rest of full
     // delta = delta' \ small run; small run' = small run u delta
-    DevBuf &jb = holder(ws, j);  // J is consumed: receives delta
     ctx.reserve(ws.small[1 - F.scur], (F.nsmall + nd1) * 8);
     const u64 n = diff_merge_words(ctx, ws.small[F.scur].as<u64>(), F.nsmall, d1buf.as<u64>(), nd1,
                                    ws.small[1 - F.scur].as<u64>(), jb.as<u64>(), Codec::Raw);
     if (n) {
         F.scur = 1 - F.scur;
         F.nsmall += n;
+        F.ssample_ok = false;
     }
     n_delta = n;
     if (F.nsmall && F.nsmall * ctx.tune.small_ratio >= F.nbig) {
@@ -361,13 +388,28 @@ u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta) {
         F.nbig += F.nsmall;
         F.nsmall = 0;
         F.sample_ok = false;
+        F.ssample_ok = false;
     }
     return jb.as<u64>();
+}
+
+// Merges the tiny run into the small run.
+void fold_tiny(Context &ctx, FullSet &F) {
+    Workspace &ws = ctx.ws;
+    if (F.ntiny == 0) return;
+    ctx.reserve(ws.small[1 - F.scur], (F.nsmall + F.ntiny) * 8);
+    merge_words(ctx, ws.small[F.scur].as<u64>(), F.nsmall, ws.tiny[F.tcur].as<u64>(), F.ntiny,
+                ws.small[1 - F.scur].as<u64>(), Codec::Raw);
+    F.scur = 1 - F.scur;
+    F.nsmall += F.ntiny;
+    F.ntiny = 0;
+    F.ssample_ok = false;
 }
 
 // Final full relation as one sorted run in ws.full[F.cur].
 void settle(Context &ctx, FullSet &F) {
     Workspace &ws = ctx.ws;
+    fold_tiny(ctx, F);
     if (F.nsmall == 0) return;
     ctx.reserve(ws.full[1 - F.cur], (F.nbig + F.nsmall) * 8);
     merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.small[F.scur].as<u64>(), F.nsmall,
@@ -395,6 +437,7 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     u64 nfull = 0;
     int cur = 0;
     FullSet F;
+    F.three = true;  // plain runs: large, small and tiny runs
     if (n > 0) {
         rank_nodes(ctx, rows, n, g);
         ctx.reserve(ws.jbuf[0], n * 8);
@@ -421,7 +464,7 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
             ndelta = nnew;
             r.deltas.push_back((i64) nnew);
             r.joins.push_back((i64) nj);
-            r.fulls.push_back((i64) (F.nbig + F.nsmall));
+            r.fulls.push_back((i64) F.size());
             if (nnew == 0) break;  // |full| unchanged
             if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
         }
@@ -522,6 +565,7 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     u64 nfull = 0;
     int cur = 0;
     FullSet F;
+    F.three = true;  // plain runs: large, small and tiny runs
     if (n > 0) {
         rank_nodes(ctx, rows, n, g);
         ctx.reserve(ws.jbuf[0], n * 8);
@@ -559,7 +603,7 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
             ndelta = nnew;
             r.deltas.push_back((i64) nnew);
             r.joins.push_back((i64) (n1 + n2));
-            r.fulls.push_back((i64) (F.nbig + F.nsmall));
+            r.fulls.push_back((i64) F.size());
             if (nnew == 0) break;
             if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
         }

@@ -56,6 +56,9 @@ struct Graph {
     int win[8] = {};
 };
 
+// The full relation of TC/SG as disjoint sorted duplicate-free runs: large
+// (ws.full[cur]), small (ws.small[scur]) and, when `three` is set, tiny
+// (ws.tiny[tcur]). A tiny run is only non-empty while the small run is.
 struct FullSet {
     int cur = 0;
     u64 nbig = 0;
@@ -63,6 +66,12 @@ struct FullSet {
     u64 nsmall = 0;
     u64 ns = 0;
     bool sample_ok = false;
+    bool three = false;       // use the tiny run
+    int tcur = 0;
+    u64 ntiny = 0;
+    u64 nss = 0;              // sample of the small run
+    bool ssample_ok = false;
+    u64 size() const { return nbig + nsmall + ntiny; }
 };
 
 
@@ -77,6 +86,7 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
 u64 *join_unsorted(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, EmitKind kind, u64 &n_j,
                    PhaseTimer &pt);
 u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta);
+void fold_tiny(Context &ctx, FullSet &F);
 void settle(Context &ctx, FullSet &F);
 
 }  // namespace detail

@@ -98,7 +98,9 @@ struct Workspace {
     DevBuf csr_off, csr_val;
     DevBuf full[2];        // full relation (large run), ping-pong
     DevBuf small[2];       // full relation (small run), ping-pong
+    DevBuf tiny[2];        // full relation (tiny run, plain runs only), ping-pong
     DevBuf sample;         // sample of the large run for sparse probes
+    DevBuf sample_small;   // sample of the small run for sparse probes
     DevBuf jbuf[2];        // join output / sort ping-pong / delta
     DevBuf offsets;        // join count offsets
     DevBuf wcc_label, wcc_flag, wcc_next;

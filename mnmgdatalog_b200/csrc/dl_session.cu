@@ -738,7 +738,8 @@ void session_destroy(SessionImpl *s) {
     for (DevBuf *b : bufs) p.give_back(*b);
     Workspace &w = c.ws;
     DevBuf *wbufs[] = {&w.input,    &w.ids,      &w.w0,       &w.w1,      &w.csr_off,  &w.csr_val,
-                       &w.full[0],  &w.full[1],  &w.small[0], &w.small[1], &w.sample,  &w.jbuf[0],
+                       &w.full[0],  &w.full[1],  &w.small[0], &w.small[1], &w.tiny[0], &w.tiny[1],
+                       &w.sample,   &w.sample_small, &w.jbuf[0],
                        &w.jbuf[1],  &w.offsets,  &w.wcc_label, &w.wcc_flag, &w.wcc_next};
     for (DevBuf *b : wbufs) p.give_back(*b);
     for (auto &b : c.spares) p.give_back(b);
@@ -1013,7 +1014,8 @@ u64 session_device_bytes(const SessionImpl &s) {
     u64 b = 0;
     const DevBuf *bufs[] = {&s.off,     &s.val,       &s.delta,    &s.label,      &s.flag,       &s.nextl,
                             &w.input,   &w.ids,       &w.w0,       &w.w1,         &w.csr_off,    &w.csr_val,
-                            &w.full[0], &w.full[1],   &w.small[0], &w.small[1],   &w.sample,     &w.jbuf[0],
+                            &w.full[0], &w.full[1],   &w.small[0], &w.small[1],   &w.tiny[0],    &w.tiny[1],
+                            &w.sample,  &w.sample_small, &w.jbuf[0],
                             &w.jbuf[1], &w.offsets,   &c.lookback, &c.radix_part, &c.lbs_splits, &c.sort_hist,
                             &c.merge_splits};
     for (const DevBuf *x : bufs) b += x->cap;  // cached spare buffers are not counted: they are free memory
