@@ -143,15 +143,18 @@ __global__ void session_hist_kernel(const u64 *__restrict__ d, u64 n, int shift,
             if (sh[i]) atomicAdd(&cnt[i], (unsigned long long) sh[i]);
 }
 
-// Word ranges of instances in the two sorted runs: for instance k (ranks
-// lohi[k] .. lohi[n + k]) out[4k..4k+3] = [first, end) in `big`, then in `small`.
-__global__ void session_bounds_kernel(const u64 *__restrict__ big, u64 nbig, const u64 *__restrict__ small,
-                                      u64 nsmall, const u64 *__restrict__ lohi, u32 n, int bits,
+// Word ranges of instances in the three sorted runs: for instance k (ranks
+// lohi[k] .. lohi[n + k]) out[6k..6k+5] = [first, end) in run 0, 1 and 2.
+struct Runs3 {
+    const u64 *w[3];
+    u64 n[3];
+};
+__global__ void session_bounds_kernel(Runs3 runs, const u64 *__restrict__ lohi, u32 n, int bits,
                                       u64 *__restrict__ out) {
-    GRID_STRIDE(t, 4 * (u64) n) {
-        const u64 k = t >> 2, which = t & 3;
+    GRID_STRIDE(t, 6 * (u64) n) {
+        const u64 k = t / 6, which = t % 6, r = which >> 1;
         const u64 target = (which & 1 ? lohi[n + k] : lohi[k]) << bits;
-        out[t] = which < 2 ? lower_bound_u64(big, nbig, target) : lower_bound_u64(small, nsmall, target);
+        out[t] = lower_bound_u64(runs.w[r], runs.n[r], target);
     }
 }
 
@@ -291,7 +294,11 @@ struct SessionImpl {
     u64 next_rank = 0;
     DevBuf off, val;  // union offset table over ranks, values
     u64 n_vals = 0;
-    FullSet F;
+    FullSet F = [] {
+        FullSet f;
+        f.three = true;
+        return f;
+    }();
     u64 dead = 0;  // words of finished instances still in the full runs
     DevBuf delta;  // union delta (probe of the next iteration)
     u64 n_delta = 0;
@@ -339,11 +346,14 @@ void full_insert_new(SessionImpl &s, const u64 *w, u64 n) {
     Workspace &ws = ctx.ws;
     FullSet &F = s.F;
     if (n == 0) return;
-    ctx.reserve(ws.small[1 - F.scur], (F.nsmall + n) * 8);
-    merge_words(ctx, ws.small[F.scur].as<u64>(), F.nsmall, w, n, ws.small[1 - F.scur].as<u64>(), Codec::Raw);
-    F.scur = 1 - F.scur;
-    F.nsmall += n;
-    if (F.nsmall * ctx.tune.small_ratio >= F.nbig) {
+    // new ranks are above every word in the runs: the merge appends
+    ctx.reserve(ws.tiny[1 - F.tcur], (F.ntiny + n) * 8);
+    merge_words(ctx, ws.tiny[F.tcur].as<u64>(), F.ntiny, w, n, ws.tiny[1 - F.tcur].as<u64>(), Codec::Raw);
+    F.tcur = 1 - F.tcur;
+    F.ntiny += n;
+    if (F.ntiny * ctx.tune.small_ratio >= F.nsmall) fold_tiny(ctx, F);  // also when the small run is empty
+    if (F.nsmall && F.nsmall * ctx.tune.small_ratio >= F.nbig) {
+        fold_tiny(ctx, F);
         ctx.reserve(ws.full[1 - F.cur], (F.nbig + F.nsmall) * 8);
         merge_words(ctx, ws.full[F.cur].as<u64>(), F.nbig, ws.small[F.scur].as<u64>(), F.nsmall,
                     ws.full[1 - F.cur].as<u64>(), Codec::Raw);
@@ -351,6 +361,7 @@ void full_insert_new(SessionImpl &s, const u64 *w, u64 n) {
         F.nbig += F.nsmall;
         F.nsmall = 0;
         F.sample_ok = false;
+        F.ssample_ok = false;
     }
 }
 
@@ -439,37 +450,72 @@ void upload_ranges(SessionImpl &s, const std::vector<i64> &ids) {
     s.ctx.sync();  // h is a host temporary
 }
 
-// Sorted words of finished TC/SG instances out of both full runs, into one
+// Sorted words of finished TC/SG instances out of the full runs, into one
 // block (each instance's words are a key range of each run).
 void extract_words(SessionImpl &s, const std::vector<i64> &ids) {
     Context &ctx = s.ctx;
     Workspace &ws = ctx.ws;
     const u64 n = ids.size();
     upload_ranges(s, ids);
-    ctx.reserve(s.counts, 4 * n * 8);
-    const u64 *big = ws.full[s.F.cur].as<u64>(), *small = ws.small[s.F.scur].as<u64>();
+    ctx.reserve(s.counts, 6 * n * 8);
+    Runs3 runs;
+    runs.w[0] = ws.full[s.F.cur].as<u64>();
+    runs.n[0] = s.F.nbig;
+    runs.w[1] = ws.small[s.F.scur].as<u64>();
+    runs.n[1] = s.F.nsmall;
+    runs.w[2] = ws.tiny[s.F.tcur].as<u64>();
+    runs.n[2] = s.F.ntiny;
     DL_LAUNCH(ctx, K_PREP, 0,
-              session_bounds_kernel<<<grid_for(4 * n, 256, ctx, 4), 256, 0, ctx.stream>>>(
-                  big, s.F.nbig, small, s.F.nsmall, s.range_lo.as<u64>(), (u32) n, s.bits, s.counts.as<u64>()));
-    std::vector<u64> hb(4 * n);
-    DL_CUDA(cudaMemcpyAsync(hb.data(), s.counts.p, 4 * n * 8, cudaMemcpyDeviceToHost, ctx.stream));
+              session_bounds_kernel<<<grid_for(6 * n, 256, ctx, 4), 256, 0, ctx.stream>>>(
+                  runs, s.range_lo.as<u64>(), (u32) n, s.bits, s.counts.as<u64>()));
+    std::vector<u64> hb(6 * n);
+    DL_CUDA(cudaMemcpyAsync(hb.data(), s.counts.p, 6 * n * 8, cudaMemcpyDeviceToHost, ctx.stream));
     ctx.sync();
-    u64 total = 0;
-    for (u64 k = 0; k < n; ++k) total += (hb[4 * k + 1] - hb[4 * k]) + (hb[4 * k + 3] - hb[4 * k + 2]);
+    u64 total = 0, pair_max = 0;
+    for (u64 k = 0; k < n; ++k) {
+        const u64 na = hb[6 * k + 1] - hb[6 * k], nb = hb[6 * k + 3] - hb[6 * k + 2], nc = hb[6 * k + 5] - hb[6 * k + 4];
+        total += na + nb + nc;
+        if (na && nb && nc) pair_max = std::max(pair_max, na + nb);
+    }
     auto block = make_block(ctx, total * 8);
+    DevBuf tmp;  // run 0 + run 1 slices of an instance that has words in all three runs
+    if (pair_max) ctx.reserve(tmp, pair_max * 8);
     u64 at = 0;
     for (u64 k = 0; k < n; ++k) {
         SessionInstance &in = s.inst[ids[k]];
-        const u64 a0 = hb[4 * k], na = hb[4 * k + 1] - a0, b0 = hb[4 * k + 2], nb = hb[4 * k + 3] - b0;
+        const u64 *src[3];
+        u64 len[3];
+        int m = 0;
+        for (int r = 0; r < 3; ++r) {
+            const u64 b = hb[6 * k + 2 * r], e = hb[6 * k + 2 * r + 1];
+            if (e > b) {
+                src[m] = runs.w[r] + b;
+                len[m] = e - b;
+                ++m;
+            }
+        }
         u64 *dst = block->as<u64>() + at;
-        if (na && nb) merge_words(ctx, big + a0, na, small + b0, nb, dst, Codec::Raw);
-        else if (na) DL_CUDA(cudaMemcpyAsync(dst, big + a0, na * 8, cudaMemcpyDeviceToDevice, ctx.stream));
-        else if (nb) DL_CUDA(cudaMemcpyAsync(dst, small + b0, nb * 8, cudaMemcpyDeviceToDevice, ctx.stream));
+        u64 cnt = 0;
+        if (m == 1) {
+            DL_CUDA(cudaMemcpyAsync(dst, src[0], len[0] * 8, cudaMemcpyDeviceToDevice, ctx.stream));
+            cnt = len[0];
+        } else if (m == 2) {
+            merge_words(ctx, src[0], len[0], src[1], len[1], dst, Codec::Raw);
+            cnt = len[0] + len[1];
+        } else if (m == 3) {
+            merge_words(ctx, src[0], len[0], src[1], len[1], tmp.as<u64>(), Codec::Raw);
+            merge_words(ctx, tmp.as<u64>(), len[0] + len[1], src[2], len[2], dst, Codec::Raw);
+            cnt = len[0] + len[1] + len[2];
+        }
         in.result_block = block;
         in.result_off = at;
-        in.n_result = na + nb;
-        at += na + nb;
-        s.dead += na + nb;
+        in.n_result = cnt;
+        at += cnt;
+        s.dead += cnt;
+    }
+    if (pair_max) {
+        ctx.sync();  // the merges that read tmp are done
+        ctx.give_back(tmp);
     }
 }
 
@@ -539,6 +585,7 @@ void reset_if_idle(SessionImpl &s) {
     s.next_rank = 0;
     s.n_vals = 0;
     s.F = FullSet();
+    s.F.three = true;
     s.dead = 0;
     s.n_delta = 0;
     s.inst_dirty = true;
@@ -560,7 +607,7 @@ struct KeepLive {
 // at least half of the full relation.
 void maybe_compact(SessionImpl &s) {
     if (s.program == DL_PROGRAM_WCC || s.active.empty()) return;
-    const u64 total = s.F.nbig + s.F.nsmall;
+    const u64 total = s.F.size();
     if (s.dead == 0 || s.dead * 2 < total) return;
     Context &ctx = s.ctx;
     Workspace &ws = ctx.ws;
@@ -568,7 +615,10 @@ void maybe_compact(SessionImpl &s) {
     KeepLive keep{s.inst_lo.as<u64>(), s.inst_hi.as<u64>(), (u32) s.active.size(), s.bits};
     s.F.nbig = session_select(ctx, ws.full[s.F.cur].as<u64>(), s.F.nbig, keep, 60);
     s.F.nsmall = session_select(ctx, ws.small[s.F.scur].as<u64>(), s.F.nsmall, keep, 60);
+    s.F.ntiny = session_select(ctx, ws.tiny[s.F.tcur].as<u64>(), s.F.ntiny, keep, 60);
     s.F.sample_ok = false;
+    s.F.ssample_ok = false;
+    if (s.F.nsmall == 0) fold_tiny(ctx, s.F);  // a tiny run needs a small run
     s.dead = 0;
 }
 
