@@ -131,7 +131,8 @@ typedef struct dl_tuning {
     int32_t small_ratio;          /* TC/SG: small run folded into the large one at |small| * ratio >= |large| (1..64, default 4) */
     int32_t sort_input_tma;       /* three-kernel pass input: 1 = TMA double buffer (default), 0 = direct loads */
     double hash_load_factor;      /* dl_build_hash_table's default load factor (0 < lf < 1, default 0.5) */
-    int32_t reserved[4];
+    int32_t join_first_pass;      /* TC: 1 = the join emit also does the sort's first radix pass (default), 0 = not */
+    int32_t reserved[3];
 } dl_tuning;
 DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out);
 DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *tuning);

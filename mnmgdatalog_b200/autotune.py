@@ -20,8 +20,9 @@ import json
 import sys
 import time
 
-SORT_VARIANTS = [  # (sort_algorithm, sort_ranking, sort_keys_per_thread, sort_input_tma)
-    (1, 1, 16, 1), (1, 1, 16, 0), (1, 0, 16, 1), (0, 1, 16, 1), (0, 0, 16, 1), (0, 1, 12, 1),
+SORT_VARIANTS = [  # (sort_algorithm, sort_ranking, sort_keys_per_thread, sort_input_tma, join_first_pass)
+    (1, 1, 16, 1, 1), (1, 1, 16, 1, 0), (1, 1, 16, 0, 1), (1, 0, 16, 1, 1), (0, 1, 16, 1, 0), (0, 0, 16, 1, 0),
+    (0, 1, 12, 1, 0),
 ]
 RATIOS = [2, 4, 8]
 LOAD_FACTORS = [0.25, 0.5, 0.7]
@@ -31,8 +32,9 @@ def candidates(stage: str, best: dict) -> list[dict]:
     """Settings to try in one coordinate-descent stage, around `best`."""
     out = []
     if stage == "sort":
-        for a, r, k, t in SORT_VARIANTS:
-            out.append(dict(best, sort_algorithm=a, sort_ranking=r, sort_keys_per_thread=k, sort_input_tma=t))
+        for a, r, k, t, f in SORT_VARIANTS:
+            out.append(dict(best, sort_algorithm=a, sort_ranking=r, sort_keys_per_thread=k, sort_input_tma=t,
+                            join_first_pass=f))
     elif stage == "dense_ratio":
         out = [dict(best, dense_ratio=v) for v in RATIOS]
     elif stage == "small_ratio":

@@ -64,7 +64,7 @@ class dl_run_info(C.Structure):
 class dl_tuning(C.Structure):
     _fields_ = [("sort_algorithm", C.c_int32), ("sort_ranking", C.c_int32), ("sort_keys_per_thread", C.c_int32),
                 ("dense_ratio", C.c_int32), ("small_ratio", C.c_int32), ("sort_input_tma", C.c_int32),
-                ("hash_load_factor", C.c_double), ("reserved", C.c_int32 * 4)]
+                ("hash_load_factor", C.c_double), ("join_first_pass", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class dl_kernel_stat(C.Structure):

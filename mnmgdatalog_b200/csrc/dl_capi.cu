@@ -611,6 +611,7 @@ DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out) {
     out->dense_ratio = (int32_t) t.dense_ratio;
     out->small_ratio = (int32_t) t.small_ratio;
     out->sort_input_tma = t.sort_tma;
+    out->join_first_pass = t.join_first_pass;
     out->hash_load_factor = t.hash_load;
     return DL_OK;
 }
@@ -623,6 +624,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     DL_REQUIRE(t->dense_ratio >= 1 && t->dense_ratio <= 64, "dense_ratio must be in 1..64");
     DL_REQUIRE(t->small_ratio >= 1 && t->small_ratio <= 64, "small_ratio must be in 1..64");
     DL_REQUIRE(t->sort_input_tma == 0 || t->sort_input_tma == 1, "sort_input_tma must be 0 or 1");
+    DL_REQUIRE(t->join_first_pass == 0 || t->join_first_pass == 1, "join_first_pass must be 0 or 1");
     DL_REQUIRE(t->hash_load_factor > 0.0 && t->hash_load_factor < 1.0, "hash_load_factor must be in (0, 1)");
     dl::Tuning &o = ctx->c.tune;
     o.sort_algo = t->sort_algorithm;
@@ -631,6 +633,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     o.dense_ratio = (u64) t->dense_ratio;
     o.small_ratio = (u64) t->small_ratio;
     o.sort_tma = t->sort_input_tma;
+    o.join_first_pass = t->join_first_pass;
     o.hash_load = t->hash_load_factor;
     return DL_OK;
 }

@@ -222,6 +222,25 @@ u64 *join_and_sort(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
     ctx.reserve(jout, std::max<u64>(total, 1) * 8);
     if (total == 0) return jout.as<u64>();
     const int key_bits = 2 * g.bits;
+    // TC words (z << bits | v) take bits 0-7 from the probe row: the emit
+    // itself groups them by that digit, and the sort starts at bit 8
+    const bool first_pass = ctx.tune.join_first_pass && kind == EmitKind::ZV && g.bits >= 8 &&
+                            !radix_wants_histogram(ctx) && (g.nwin == 0 || g.win[0] == 0);
+    if (first_pass) {
+        join_emit_bucketed(ctx, g.csr, probe, n_probe, g.bits, ws.offsets.as<u64>(), total, jout.as<u64>());
+        pt.mark(PH_DEDUP);
+        DevBuf &pbuf = holder(ws, probe);
+        u64 *jptr = jout.as<u64>();
+        ctx.reserve(pbuf, total * 8);  // probe is dead now
+        int w[8];
+        int nw = 0;
+        if (g.nwin) {
+            for (int i = 1; i < g.nwin; ++i) w[nw++] = g.win[i];
+        } else {
+            for (int sh = 8; sh < key_bits; sh += 8) w[nw++] = sh;
+        }
+        return radix_sort_windows(ctx, jptr, pbuf.as<u64>(), total, w, nw);
+    }
     const bool fuse_hist = radix_wants_histogram(ctx) && !g.nwin;
     const int ndig = fuse_hist ? (key_bits + 7) / 8 : 0;
     u64 *hist = fuse_hist ? radix_hist_buffer(ctx) : nullptr;

@@ -108,12 +108,13 @@ struct Workspace {
 
 // Engine knobs the autotuner sets per context (mnmgdatalog_b200/autotune.py);
 // the defaults are the measured best on B200. DL_SORT_ALGO, DL_SORT_RANK,
-// DL_SORT_KPT and DL_SORT_TMA override the sort defaults.
+// DL_SORT_KPT, DL_SORT_TMA and DL_JOIN_FIRST_PASS override the defaults.
 struct Tuning {
     int sort_algo = 1;          // 1 = three-kernel LSD pass, 0 = onesweep
     int rank = 1;               // 1 = shared-memory peer masks, 0 = warp ballots
     int sort_kpt = 16;          // onesweep keys per thread: 12 or 16
     int sort_tma = 1;           // three-kernel pass input: 1 = TMA double buffer, 0 = direct loads
+    int join_first_pass = 1;    // 1 = TC join emit does the first radix pass (bits 0-7), 0 = separate pass
     u64 dense_ratio = 4;        // fused full rewrite when |J| * dense_ratio >= |large run|
     u64 small_ratio = 4;        // small run folded when |small| * small_ratio >= |large run|
     double hash_load = 0.5;     // default load factor of dl_build_hash_table
@@ -133,6 +134,7 @@ struct Context {
     DevBuf lbs_splits;              // join emit partition points
     DevBuf radix_part;              // per-(digit, CTA) counts and offsets of a radix pass
     DevBuf merge_splits;            // merge-path split points of a set operation
+    DevBuf bucket_cursor;           // per-digit output cursors of the bucketed join emit
     u64 *host_scalars = nullptr;    // pinned mirror for small D2H reads
     Workspace ws;
     u64 run_join_total = 0, run_join_max = 0;  // join statistics of the current run

@@ -50,6 +50,32 @@ void join_emit(Context &ctx, const Csr &csr, const u64 *probe, u64 n_probe, int 
     }
 }
 
+void join_emit_bucketed(Context &ctx, const Csr &csr, const u64 *probe, u64 n_probe, int bits, const u64 *offsets,
+                        u64 total, u64 *out) {
+    if (total == 0) return;
+    if (bits < 8) throw Error(DL_ERR_INTERNAL, "bucketed emit needs 8 payload bits");
+    const CsrSrc<EmitKind::ZV> src{csr.off, csr.val, probe, bits};
+    ctx.reserve(ctx.bucket_cursor, 256 * sizeof(u64));
+    auto *cur = ctx.bucket_cursor.as<unsigned long long>();
+    DL_CUDA(cudaMemsetAsync(cur, 0, 256 * sizeof(u64), ctx.stream));
+    const unsigned hg = (unsigned) std::max<u64>(1, std::min<u64>((n_probe + 255) / 256, (u64) ctx.sm_count * 8));
+    DL_LAUNCH(ctx, K_JOIN_COUNT, 8.0 * n_probe,
+              digit0_hist_kernel<CsrSrc<EmitKind::ZV>><<<hg, 256, 0, ctx.stream>>>(src, probe, n_probe, cur));
+    DL_LAUNCH(ctx, K_JOIN_PARTITION, 0, bucket_starts_kernel<<<1, 256, 0, ctx.stream>>>(cur));
+    const u64 tiles = (n_probe + total + JN_TILE - 1) / JN_TILE;
+    ctx.lbs_splits.reserve((tiles + 1) * sizeof(u64));
+    u64 *splits = ctx.lbs_splits.as<u64>();
+    DL_LAUNCH(ctx, K_JOIN_PARTITION, 0,
+              lbs_partition_kernel<<<(unsigned) ((tiles + 1 + 255) / 256), 256, 0, ctx.stream>>>(offsets, n_probe, total,
+                                                                                                 tiles + 1, splits));
+    auto kern = join_emit_bucket_kernel<CsrSrc<EmitKind::ZV>>;
+    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(JoinBucketSmem)));
+    DL_LAUNCH(ctx, K_JOIN_EMIT, CsrSrc<EmitKind::ZV>::prof_bytes(n_probe, total),
+              kern<<<(unsigned) tiles, JN_THREADS, sizeof(JoinBucketSmem), ctx.stream>>>(src, n_probe, offsets, total,
+                                                                                          splits, out, cur,
+                                                                                          &ctx.ctrl->err));
+}
+
 // ---- C-ABI hash table ------------------------------------------------------
 
 namespace {

@@ -229,6 +229,128 @@ join_emit_kernel(Src src, u64 n_probe, const u64 *__restrict__ offsets, u64 tota
     }
 }
 
+// Join emit fused with the first LSD radix pass (bits 0-7 of the output
+// words), for sources whose output words take their low byte from the probe
+// row (CsrSrc<ZV> with bits >= 8: (z << bits) | v). The first pass of an LSD
+// sort needs no stability -- there is no earlier order to keep -- so a tile
+// ranks its words per digit with shared-memory atomics, reserves each
+// digit's range with one atomic on a global cursor (cursor[d] starts at the
+// digit's bucket start, from digit0_hist_kernel), stages the words grouped by
+// digit and writes every run with consecutive stores.
+struct JoinBucketSmem {
+    u64 obeg[JN_TILE + 1];
+    u64 begin[JN_TILE + 1];  // first match of each row; then the staged words
+    u32 payload[JN_TILE + 1];
+    u32 cnt[256];
+    u32 pre[256];
+    u64 base[256];
+    u32 scratch[JN_THREADS / 32 + 1];
+};
+
+template <class Src>
+__global__ void __launch_bounds__(JN_THREADS)
+join_emit_bucket_kernel(Src src, u64 n_probe, const u64 *__restrict__ offsets, u64 total,
+                        const u64 *__restrict__ splits, u64 *__restrict__ out,
+                        unsigned long long *__restrict__ cursor, u32 *err) {
+    static_assert(JN_THREADS == 256, "one thread per digit");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    JoinBucketSmem &s = *reinterpret_cast<JoinBucketSmem *>(smem_raw);
+    constexpr u32 VT = JN_TILE / JN_THREADS;
+    const int tid = threadIdx.x;
+    const u64 tile = blockIdx.x;
+    const u64 d0 = tile * JN_TILE;
+    const u64 d1 = min(d0 + JN_TILE, n_probe + total);
+    const u64 i0 = splits[tile], i1 = splits[tile + 1];
+    const u64 o0 = d0 - i0, o1 = d1 - i1;
+    const u64 istart = i0 > 0 ? i0 - 1 : 0;
+    const u32 ni = (u32) (i1 - istart);
+    const u32 no = (u32) (o1 - o0);
+    s.cnt[tid] = 0;
+    for (u32 j = tid; j < ni; j += JN_THREADS) {
+        const u64 gi = istart + j;
+        u64 begin, payload;
+        src.item(gi, begin, payload);
+        s.obeg[j] = offsets[gi];
+        s.begin[j] = begin;
+        s.payload[j] = payload;
+    }
+    __syncthreads();
+    u64 wv[VT];
+    u32 rk[VT];
+    u32 j = 0;
+#pragma unroll
+    for (u32 k = 0; k < VT; ++k) {
+        wv[k] = 0;
+        rk[k] = 0;
+        const u64 o = o0 + tid + (u64) k * JN_THREADS;
+        if (o < o1) {
+            u32 lo = j, hi = ni;  // owner: last loaded row whose first output is <= o
+            while (lo < hi) {
+                const u32 mid = (lo + hi) >> 1;
+                if (s.obeg[mid] <= o) lo = mid + 1;
+                else hi = mid;
+            }
+            j = lo - 1;
+            const u64 w = src.word(s.begin[j] + (o - s.obeg[j]), s.payload[j]);
+            wv[k] = w;
+            rk[k] = atomicAdd(&s.cnt[w & 255u], 1u);
+        }
+    }
+    __syncthreads();  // counts complete; s.begin no longer read
+    u32 tot;
+    const u32 c = s.cnt[tid];
+    const u32 pre = block_exclusive_sum<JN_THREADS / 32>(c, s.scratch, &tot);
+    s.pre[tid] = pre;
+    if (c) s.base[tid] = (u64) atomicAdd(&cursor[tid], (unsigned long long) c) - pre;
+    __syncthreads();
+#pragma unroll
+    for (u32 k = 0; k < VT; ++k) {
+        const u64 o = o0 + tid + (u64) k * JN_THREADS;
+        if (o < o1) s.begin[s.pre[wv[k] & 255u] + rk[k]] = wv[k];
+    }
+    __syncthreads();
+    for (u32 i = tid; i < no; i += JN_THREADS) {
+        const u64 w = s.begin[i];
+        const u64 pos = s.base[w & 255u] + i;
+        if (pos < total) out[pos] = w;
+        else atomicOr(err, DL_DEVERR_CAPACITY);  // histogram and emit disagree: reported, never written
+    }
+}
+
+// Degree-weighted histogram of the probe rows' low byte: the number of join
+// output words per value of their bits 0-7 (for sources like the above).
+template <class Src>
+__global__ void __launch_bounds__(256) digit0_hist_kernel(Src src, const u64 *__restrict__ probe, u64 n,
+                                                          unsigned long long *__restrict__ hist) {
+    __shared__ unsigned long long h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64) gridDim.x * blockDim.x) {
+        const u64 deg = src.degree(i);
+        if (deg) atomicAdd(&h[probe[i] & 255u], (unsigned long long) deg);
+    }
+    __syncthreads();
+    if (h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+}
+
+// hist[0..255] -> exclusive prefix (the digits' bucket starts), in place.
+static __global__ void __launch_bounds__(256) bucket_starts_kernel(unsigned long long *hist) {
+    __shared__ unsigned long long part[256 / 32];
+    const u32 lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned long long v = hist[threadIdx.x];
+    unsigned long long x = v;  // inclusive warp scan
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= (u32) d) x += y;
+    }
+    if (lane == 31) part[w] = x;
+    __syncthreads();
+    unsigned long long before = 0;
+    for (u32 i = 0; i < w; ++i) before += part[i];
+    hist[threadIdx.x] = before + x - v;
+}
+
 static __global__ void lbs_partition_kernel(const u64 *__restrict__ offsets, u64 n, u64 total, u64 n_splits,
                                      u64 *__restrict__ splits) {
     const u64 t = (u64) blockIdx.x * blockDim.x + threadIdx.x;
@@ -281,6 +403,11 @@ void emit_matches(Context &ctx, const Src &src, u64 n, const u64 *offsets, u64 t
     DL_LAUNCH(ctx, Src::kProfKind, Src::prof_bytes(n, total), kern<<<(unsigned) tiles, JN_THREADS, sizeof(JoinSmem), ctx.stream>>>(src, n, offsets, total, splits, out, hist,
                                                                          ndig, self_pairs));
 }
+
+// Join of probe rows against the CSR (EmitKind::ZV, bits >= 8) with the
+// output already grouped by bits 0-7 of its words (the first LSD pass).
+void join_emit_bucketed(Context &ctx, const Csr &csr, const u64 *probe, u64 n_probe, int bits, const u64 *offsets,
+                        u64 total, u64 *out);
 
 HashTable *hash_table_build(Context &ctx, const u64 *rel, u64 n, double load_factor);
 u64 hash_join_count(Context &ctx, const HashTable &ht, const u64 *probe, u64 n, u64 *offsets);

@@ -199,6 +199,8 @@ Tuning default_tuning() {
         if (e && std::string(e) == "onesweep") d.sort_algo = 0;
         e = getenv("DL_SORT_TMA");
         if (e && std::string(e) == "0") d.sort_tma = 0;
+        e = getenv("DL_JOIN_FIRST_PASS");
+        if (e && std::string(e) == "0") d.join_first_pass = 0;
         return d;
     }();
     return t;

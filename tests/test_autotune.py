@@ -2,12 +2,13 @@
 from mnmgdatalog_b200 import autotune
 
 BASE = {"sort_algorithm": 1, "sort_ranking": 1, "sort_keys_per_thread": 16, "sort_input_tma": 1, "dense_ratio": 4,
-        "small_ratio": 4, "hash_load_factor": 0.5}
+        "small_ratio": 4, "hash_load_factor": 0.5, "join_first_pass": 1}
 
 
 def test_sort_stage_covers_every_variant_once():
     c = autotune.candidates("sort", BASE)
-    keys = [(x["sort_algorithm"], x["sort_ranking"], x["sort_keys_per_thread"], x["sort_input_tma"]) for x in c]
+    keys = [(x["sort_algorithm"], x["sort_ranking"], x["sort_keys_per_thread"], x["sort_input_tma"],
+             x["join_first_pass"]) for x in c]
     assert sorted(keys) == sorted(autotune.SORT_VARIANTS)
     assert all(x["dense_ratio"] == 4 and x["hash_load_factor"] == 0.5 for x in c)
 

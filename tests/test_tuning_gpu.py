@@ -18,7 +18,7 @@ def test_tuning_round_trip_and_validation(engine):
         t = engine.tuning()
         assert (t["dense_ratio"], t["small_ratio"], t["hash_load_factor"]) == (8, 2, 0.7)
         for bad in ({"dense_ratio": 0}, {"small_ratio": 65}, {"sort_algorithm": 2}, {"sort_keys_per_thread": 8},
-                    {"hash_load_factor": 1.0}, {"sort_input_tma": 2}):
+                    {"hash_load_factor": 1.0}, {"sort_input_tma": 2}, {"join_first_pass": 3}):
             with pytest.raises(DatalogError):
                 engine.set_tuning(**bad)
         with pytest.raises(DatalogError):
@@ -34,7 +34,8 @@ def test_results_do_not_depend_on_tuning(engine, variant, ratios):
     before = engine.tuning()
     try:
         engine.set_tuning(sort_algorithm=variant[0], sort_ranking=variant[1], sort_keys_per_thread=variant[2],
-                          sort_input_tma=variant[3], dense_ratio=ratios[0], small_ratio=ratios[1])
+                          sort_input_tma=variant[3], join_first_pass=variant[4], dense_ratio=ratios[0],
+                          small_ratio=ratios[1])
         for fname, rec in EXP["inputs"].items():
             e = load_input(fname)
             for prog in ("tc", "sg"):
