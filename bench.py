@@ -60,7 +60,8 @@ def describe(config: str, edges: np.ndarray) -> dict:
     d = {"c1_tc_chung_lu": "TC, Chung-Lu n=317000 gamma=2.5 m=1050000 (each edge once, seed 0)",
          "c0_tc_dag": "TC, DAG n=5000 p=0.7 + 2000 short edges (seed 0)",
          "c2_sg_lattice": "SG, 55^3 lattice 6-neighbour p=0.15 + 1% long edges (seed 0)",
-         "p1_tc_chung_lu_small": "TC, Chung-Lu n=40000 gamma=2.5 m=132500 (each edge once, seed 0)"}
+         "p1_tc_chung_lu_small": "TC, Chung-Lu n=40000 gamma=2.5 m=132500 (each edge once, seed 0)",
+         "p2_tc_chung_lu_medium": "TC, Chung-Lu n=80000 gamma=2.5 m=265000 (each edge once, seed 0)"}
     return {"workload": d.get(config, config), "config": config, "input_rows": int(len(edges))}
 
 
@@ -454,7 +455,7 @@ def main(argv=None) -> int:
     ap.add_argument("--config", default="c1_tc_chung_lu")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--dedup", choices=["auto", "sort", "hash"], default="auto",
+    ap.add_argument("--dedup", choices=["auto", "sort", "hash", "bitmap"], default="auto",
                     help="how TC removes known tuples (same results)")
     ap.add_argument("--batch-instances", type=int, default=1024, help="batched form instances (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=600, help="served form requests (0: skip)")

@@ -78,11 +78,15 @@ typedef enum dl_wcc_stop {
 
 /* How TC removes known tuples from a join output (same results either way). */
 typedef enum dl_dedup {
-    DL_DEDUP_AUTO = 0,  /* the engine's choice (currently SORT) */
+    DL_DEDUP_AUTO = 0,  /* the engine's choice: BITMAP for TC when the bit matrix and its transpose
+                           fit in dl_tuning.bitmap_max_gib and half the free device memory, else SORT */
     DL_DEDUP_SORT = 1,  /* radix sort of the join output + merge-path difference against sorted full */
-    DL_DEDUP_HASH = 2   /* full as a hash set of tuple words; one sort of the result at the end
+    DL_DEDUP_HASH = 2,  /* full as a hash set of tuple words; one sort of the result at the end
                            (no per-iteration sort, but random-access bound: 1.7x slower on
                            the 1.9e9-tuple TC benchmark) */
+    DL_DEDUP_BITMAP = 3 /* full as an n x n bit matrix over node ranks (n = distinct node ids):
+                           each join word is one atomic test-and-set, no sort or merge per
+                           iteration; needs 2 * n * n / 8 bytes (12.6 GB each for 317K nodes) */
 } dl_dedup;
 
 typedef struct dl_options {
@@ -132,7 +136,8 @@ typedef struct dl_tuning {
     int32_t sort_input_tma;       /* three-kernel pass input: 1 = TMA double buffer (default), 0 = direct loads */
     double hash_load_factor;      /* dl_build_hash_table's default load factor (0 < lf < 1, default 0.5) */
     int32_t join_first_pass;      /* TC: 1 = the join emit also does the sort's first radix pass (default), 0 = not */
-    int32_t reserved[3];
+    int32_t bitmap_max_gib;       /* TC dedup AUTO: largest bit matrix + transpose, GiB (0..1024, default 48; 0 = never) */
+    int32_t reserved[2];
 } dl_tuning;
 DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out);
 DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *tuning);

@@ -20,7 +20,7 @@ STATUS_NAMES = {
 
 PROGRAM_TC, PROGRAM_SG, PROGRAM_WCC, PROGRAM_SINGLE_JOIN = 0, 1, 2, 3
 WCC_STOP_REFERENCE, WCC_STOP_FIXPOINT = 0, 1
-DEDUP_AUTO, DEDUP_SORT, DEDUP_HASH = 0, 1, 2
+DEDUP_AUTO, DEDUP_SORT, DEDUP_HASH, DEDUP_BITMAP = 0, 1, 2, 3
 
 # Every symbol include/mnmgdl.h declares (checked by the CPU test suite).
 EXPORTS = (
@@ -64,7 +64,8 @@ class dl_run_info(C.Structure):
 class dl_tuning(C.Structure):
     _fields_ = [("sort_algorithm", C.c_int32), ("sort_ranking", C.c_int32), ("sort_keys_per_thread", C.c_int32),
                 ("dense_ratio", C.c_int32), ("small_ratio", C.c_int32), ("sort_input_tma", C.c_int32),
-                ("hash_load_factor", C.c_double), ("join_first_pass", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("hash_load_factor", C.c_double), ("join_first_pass", C.c_int32), ("bitmap_max_gib", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class dl_kernel_stat(C.Structure):

@@ -367,7 +367,7 @@ DL_API dl_status dl_run_program(dl_context *ctx, int32_t program, const int32_t 
     dl_options o{};
     if (opts) o = *opts;
     DL_REQUIRE(o.wcc_stop == DL_WCC_STOP_REFERENCE || o.wcc_stop == DL_WCC_STOP_FIXPOINT, "unknown wcc_stop");
-    DL_REQUIRE(o.dedup >= DL_DEDUP_AUTO && o.dedup <= DL_DEDUP_HASH, "unknown dedup mode");
+    DL_REQUIRE(o.dedup >= DL_DEDUP_AUTO && o.dedup <= DL_DEDUP_BITMAP, "unknown dedup mode");
     auto run = std::make_unique<dl_run>();
     dl_status st = guarded([&] {
         set_device(ctx);
@@ -456,7 +456,7 @@ DL_API dl_status dl_session_create(dl_context *ctx, int32_t program, const dl_op
     dl_options o{};
     if (opts) o = *opts;
     DL_REQUIRE(o.wcc_stop == DL_WCC_STOP_REFERENCE || o.wcc_stop == DL_WCC_STOP_FIXPOINT, "unknown wcc_stop");
-    DL_REQUIRE(o.dedup >= DL_DEDUP_AUTO && o.dedup <= DL_DEDUP_HASH, "unknown dedup mode");
+    DL_REQUIRE(o.dedup >= DL_DEDUP_AUTO && o.dedup <= DL_DEDUP_BITMAP, "unknown dedup mode");
     auto s = std::make_unique<dl_session>();
     s->ctx = ctx;
     dl_status st = guarded([&] {
@@ -613,6 +613,7 @@ DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out) {
     out->sort_input_tma = t.sort_tma;
     out->join_first_pass = t.join_first_pass;
     out->hash_load_factor = t.hash_load;
+    out->bitmap_max_gib = t.bitmap_max_gib;
     return DL_OK;
 }
 
@@ -626,6 +627,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     DL_REQUIRE(t->sort_input_tma == 0 || t->sort_input_tma == 1, "sort_input_tma must be 0 or 1");
     DL_REQUIRE(t->join_first_pass == 0 || t->join_first_pass == 1, "join_first_pass must be 0 or 1");
     DL_REQUIRE(t->hash_load_factor > 0.0 && t->hash_load_factor < 1.0, "hash_load_factor must be in (0, 1)");
+    DL_REQUIRE(t->bitmap_max_gib >= 0 && t->bitmap_max_gib <= 1024, "bitmap_max_gib must be in 0..1024");
     dl::Tuning &o = ctx->c.tune;
     o.sort_algo = t->sort_algorithm;
     o.rank = t->sort_ranking;
@@ -635,6 +637,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     o.sort_tma = t->sort_input_tma;
     o.join_first_pass = t->join_first_pass;
     o.hash_load = t->hash_load_factor;
+    o.bitmap_max_gib = t->bitmap_max_gib;
     return DL_OK;
 }
 

@@ -116,6 +116,7 @@ void Context::release_all() {
     DevBuf *all[] = {&ws.input, &ws.ids, &ws.w0, &ws.w1, &ws.csr_off, &ws.csr_val, &ws.full[0], &ws.full[1],
                      &ws.small[0], &ws.small[1], &ws.tiny[0], &ws.tiny[1], &ws.sample, &ws.sample_small,
                      &ws.jbuf[0], &ws.jbuf[1], &ws.offsets, &ws.wcc_label, &ws.wcc_flag, &ws.wcc_next,
+                     &ws.bitmat[0], &ws.bitmat[1], &ws.offsets_next,
                      &lookback, &sort_hist, &lbs_splits, &radix_part, &merge_splits, &bucket_cursor};
     for (DevBuf *b : all) b->release();
 }
@@ -156,7 +157,7 @@ const char *kernel_name(int kid) {
     static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_spine_scan", "sort_scatter_pass",
                                          "select_compact", "join_count_scan", "join_partition", "join_emit",
                                          "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build",
-                                         "sparse_diff", "hash_insert", "host_cudaMalloc", "host_cudaFree",
+                                         "sparse_diff", "hash_insert", "bitmap_expand", "bitmap_extract", "host_cudaMalloc", "host_cudaFree",
                                          "host_sync"};
     return (kid >= 0 && kid < K_COUNT) ? names[kid] : "?";
 }

@@ -466,30 +466,35 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         u64 ne;
         u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, n, 2 * g.bits, ne);
         build_csr(ctx, e, ne, g);
-        u64 nd;
-        u64 *d = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * g.bits, nd);  // tc.cu:178-181
-        ctx.reserve(ws.full[0], nd * 8);
-        DL_CUDA(cudaMemcpyAsync(ws.full[0].p, d, nd * 8, cudaMemcpyDeviceToDevice, ctx.stream));  // tc.cu:188-189
-        F.cur = 0;
-        F.nbig = nd;
-        u64 *delta = d;
-        u64 ndelta = nd;
-        for (int it = 0;; ++it) {  // tc.cu:216-314
-            u64 nj = 0;
-            u64 *j = join_and_sort(ctx, g, delta, ndelta, EmitKind::ZV, nj, nullptr, pt);
-            pt.mark(PH_MERGE);
-            u64 nnew = 0;
-            delta = absorb(ctx, F, j, nj, nnew);
-            ndelta = nnew;
-            r.deltas.push_back((i64) nnew);
-            r.joins.push_back((i64) nj);
-            r.fulls.push_back((i64) F.size());
-            if (nnew == 0) break;  // |full| unchanged
-            if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
+        if (bitmat_choose(ctx, opt, g.n_ids)) {
+            nfull = tc_bitmap_fixpoint(ctx, r, g, e, ne, opt, pt);  // result in ws.full[0]
+            cur = 0;
+        } else {
+            u64 nd;
+            u64 *d = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * g.bits, nd);  // tc.cu:178-181
+            ctx.reserve(ws.full[0], nd * 8);
+            DL_CUDA(cudaMemcpyAsync(ws.full[0].p, d, nd * 8, cudaMemcpyDeviceToDevice, ctx.stream));  // tc.cu:188-189
+            F.cur = 0;
+            F.nbig = nd;
+            u64 *delta = d;
+            u64 ndelta = nd;
+            for (int it = 0;; ++it) {  // tc.cu:216-314
+                u64 nj = 0;
+                u64 *j = join_and_sort(ctx, g, delta, ndelta, EmitKind::ZV, nj, nullptr, pt);
+                pt.mark(PH_MERGE);
+                u64 nnew = 0;
+                delta = absorb(ctx, F, j, nj, nnew);
+                ndelta = nnew;
+                r.deltas.push_back((i64) nnew);
+                r.joins.push_back((i64) nj);
+                r.fulls.push_back((i64) F.size());
+                if (nnew == 0) break;  // |full| unchanged
+                if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
+            }
+            settle(ctx, F);
+            nfull = F.nbig;
+            cur = F.cur;
         }
-        settle(ctx, F);
-        nfull = F.nbig;
-        cur = F.cur;
     }
     pt.mark(PH_FINAL);
     DL_CUDA(cudaEventRecord(ev.b, ctx.stream));

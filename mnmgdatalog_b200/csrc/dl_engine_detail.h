@@ -2,6 +2,7 @@
 // multi-instance session (dl_session.cu).
 #pragma once
 
+#include "dl_engine.h"
 #include "dl_internal.h"
 
 namespace dl {
@@ -88,6 +89,12 @@ u64 *join_unsorted(Context &ctx, const Graph &g, const u64 *probe, u64 n_probe, 
 u64 *absorb(Context &ctx, FullSet &F, u64 *j, u64 nj, u64 &n_delta);
 void fold_tiny(Context &ctx, FullSet &F);
 void settle(Context &ctx, FullSet &F);
+
+// TC with full as an n x n bit matrix (dl_bitmap.cu).
+u64 bitmat_bytes(u64 n);
+bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n);
+u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u64 ne, const dl_options &opt,
+                       PhaseTimer &pt);
 
 }  // namespace detail
 }  // namespace dl

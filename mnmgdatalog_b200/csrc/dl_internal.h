@@ -75,6 +75,9 @@ enum KernelId : int {
     K_HASH_BUILD,      // C-ABI hash table insert / value extraction
     K_SPARSE_DIFF,     // sparse set difference probes (+ run sampling)
     K_HASH_INSERT,     // hash-set dedup: 8 B read + 32 B probe sector per word, 40 B per new word
+    K_BITMAP_EXPAND,   // bit-matrix TC step: 8 B per delta row + 4 B edge value + 8 B bit-word update per
+                       // join word + 8 B per new word
+    K_BITMAP_EXTRACT,  // bit-matrix transpose, row counts, scan and word extraction of the result
     // host-side costs, counted with or without profiling (seconds = host wall time)
     K_HOST_MALLOC,     // cudaMalloc of a buffer that had to grow (bytes = size)
     K_HOST_FREE,       // cudaFree of a cached buffer dropped from the cache
@@ -103,7 +106,9 @@ struct Workspace {
     DevBuf sample_small;   // sample of the small run for sparse probes
     DevBuf jbuf[2];        // join output / sort ping-pong / delta
     DevBuf offsets;        // join count offsets
+    DevBuf offsets_next;   // bit-matrix TC: the next delta's join offsets
     DevBuf wcc_label, wcc_flag, wcc_next;
+    DevBuf bitmat[2];      // TC full relation as a bit matrix; its transpose
 };
 
 // Engine knobs the autotuner sets per context (mnmgdatalog_b200/autotune.py);
@@ -118,6 +123,7 @@ struct Tuning {
     u64 dense_ratio = 4;        // fused full rewrite when |J| * dense_ratio >= |large run|
     u64 small_ratio = 4;        // small run folded when |small| * small_ratio >= |large run|
     double hash_load = 0.5;     // default load factor of dl_build_hash_table
+    int bitmap_max_gib = 48;    // TC dedup AUTO: bit matrix and transpose at most this many GiB (0 = never)
 };
 Tuning default_tuning();
 

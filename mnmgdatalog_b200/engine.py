@@ -135,7 +135,7 @@ class Engine:
         check(lib().dl_context_synchronize(self.ctx))
 
     TUNING_FIELDS = ("sort_algorithm", "sort_ranking", "sort_keys_per_thread", "sort_input_tma", "dense_ratio",
-                     "small_ratio", "hash_load_factor", "join_first_pass")
+                     "small_ratio", "hash_load_factor", "join_first_pass", "bitmap_max_gib")
 
     def tuning(self) -> dict:
         """The context's engine knobs (dl_tuning)."""
@@ -188,7 +188,8 @@ class Engine:
         opts.wcc_stop = {"reference": capi.WCC_STOP_REFERENCE, "fixpoint": capi.WCC_STOP_FIXPOINT}[wcc_stop]
         opts.max_iterations = max_iterations
         opts.phase_timing = 1 if phase_timing else 0
-        opts.dedup = {"auto": capi.DEDUP_AUTO, "sort": capi.DEDUP_SORT, "hash": capi.DEDUP_HASH}[dedup]
+        opts.dedup = {"auto": capi.DEDUP_AUTO, "sort": capi.DEDUP_SORT, "hash": capi.DEDUP_HASH,
+                      "bitmap": capi.DEDUP_BITMAP}[dedup]
         keep = None
         if isinstance(edges, torch.Tensor) and edges.is_cuda:
             keep = _check_rel(edges) if edges.numel() else edges

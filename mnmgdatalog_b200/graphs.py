@@ -132,6 +132,9 @@ CONFIGS = {
     # the TC-at-scale shape at 1/8 of the nodes (~3e7 closure tuples, a few
     # hundred MB: larger than L2, small enough for detailed counter captures)
     "p1_tc_chung_lu_small": ("tc", chung_lu, {"n": 40_000, "m": 132_500}),
+    # 1/4 of the nodes (~1e8 closure tuples, ~4 GB on the device): join steps
+    # of milliseconds for counter captures of the bit-matrix step
+    "p2_tc_chung_lu_medium": ("tc", chung_lu, {"n": 80_000, "m": 265_000}),
 }
 
 

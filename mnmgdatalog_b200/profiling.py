@@ -27,7 +27,12 @@ CLASSES = [
     (r"radix_bucket_kernel", "sort_spine_scan"),
     (r"scan_kernel<.*DegreeOp", "join_count_scan"),
     (r"join_emit_kernel<.*WccSrc", "wcc_propagate"),
-    (r"join_emit_kernel", "join_emit"),
+    (r"join_emit_kernel|join_emit_bucket_kernel", "join_emit"),
+    (r"digit0_hist_kernel", "join_count_scan"),
+    (r"bucket_starts_kernel", "join_partition"),
+    (r"bitmat_expand_kernel|bitmat_set_kernel", "bitmap_expand"),
+    (r"bitmat_transpose_kernel|bitmat_row_count_kernel|bitmat_extract_kernel|scan_kernel<.*CountValue",
+     "bitmap_extract"),
     (r"lbs_partition_kernel", "join_partition"),
     (r"select_kernel", "select_compact"),
     (r"merge_partition_kernel", "merge_partition"),

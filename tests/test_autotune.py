@@ -2,7 +2,7 @@
 from mnmgdatalog_b200 import autotune
 
 BASE = {"sort_algorithm": 1, "sort_ranking": 1, "sort_keys_per_thread": 16, "sort_input_tma": 1, "dense_ratio": 4,
-        "small_ratio": 4, "hash_load_factor": 0.5, "join_first_pass": 1}
+        "small_ratio": 4, "hash_load_factor": 0.5, "join_first_pass": 1, "bitmap_max_gib": 48}
 
 
 def test_sort_stage_covers_every_variant_once():

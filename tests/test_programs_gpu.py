@@ -117,9 +117,9 @@ TC_FILES = [f for f, e in EXP["inputs"].items() if "tc" in e]
 
 
 @pytest.mark.parametrize("fname", TC_FILES)
-@pytest.mark.parametrize("dedup", ["sort", "hash"])
+@pytest.mark.parametrize("dedup", ["sort", "hash", "bitmap"])
 def test_tc_dedup_modes(engine, fname, dedup):
-    """Both ways of removing known tuples give the reference's rows, iteration
+    """Every way of removing known tuples gives the reference's rows, iteration
     count and per-iteration deltas."""
     e = load_input(fname)
     rec = EXP["inputs"][fname]["tc"]
@@ -129,7 +129,7 @@ def test_tc_dedup_modes(engine, fname, dedup):
     assert sha_rows(r.rows) == rec["rows_sha256"]
 
 
-@pytest.mark.parametrize("dedup", ["sort", "hash"])
+@pytest.mark.parametrize("dedup", ["sort", "hash", "bitmap"])
 def test_tc_dedup_modes_edge_cases(engine, dedup):
     for name, e in _edge_cases():
         got = engine.tc(e, dedup=dedup)
@@ -144,6 +144,32 @@ def test_tc_dedup_modes_agree_at_scale(engine):
     import torch
     e = torch.from_numpy(graphs.chung_lu(n=40_000, m=132_500, seed=0)).cuda()
     a = engine.tc(e, dedup="sort", output="device")
-    b = engine.tc(e, dedup="hash", output="device")
-    assert a.iterations == b.iterations and a.deltas.tolist() == b.deltas.tolist()
-    assert torch.equal(a.rows, b.rows)
+    for mode in ("hash", "bitmap"):
+        b = engine.tc(e, dedup=mode, output="device")
+        assert a.iterations == b.iterations and a.deltas.tolist() == b.deltas.tolist(), mode
+        assert a.join_rows_total == b.join_rows_total, mode
+        assert torch.equal(a.rows, b.rows), mode
+
+
+def test_tc_bitmap_max_iterations_and_selection(engine):
+    """The bit-matrix path stops where the sort path stops, and AUTO picks it
+    only while tuning allows (bitmap_max_gib = 0 turns it off)."""
+    from mnmgdatalog_b200 import graphs
+    e = graphs.chung_lu(n=6000, m=20000, seed=5)
+    for k in (1, 2, 5):
+        a = engine.tc(e, dedup="sort", max_iterations=k)
+        b = engine.tc(e, dedup="bitmap", max_iterations=k)
+        assert a.deltas.tolist() == b.deltas.tolist() and np.array_equal(a.rows, b.rows), k
+    before = engine.tuning()
+    try:
+        for gib, used in ((48, True), (0, False)):
+            engine.set_tuning(bitmap_max_gib=gib)
+            engine.profile(True)
+            r = engine.tc(e)
+            prof = engine.profile_read()
+            engine.profile(False)
+            assert (prof.get("bitmap_expand", {}).get("launches", 0) > 0) == used, gib
+            assert (prof.get("diff_merge", {}).get("launches", 0) > 0) != used, gib
+            assert np.array_equal(r.rows, engine.tc(e, dedup="sort").rows)
+    finally:
+        engine.set_tuning(before)
