@@ -51,10 +51,11 @@ __global__ void swap_fields_kernel(const u64 *__restrict__ in, u64 n, int bits, 
 struct StepSmem {
     u64 obeg[JN_TILE + 1];    // first output of each loaded row; then the staged words' next offsets
     u64 begin[JN_TILE + 1];   // first match of each loaded row; then the staged new words
-    u32 payload[JN_TILE + 1];
+    u32 payload[JN_TILE + 1]; // probe value of each loaded row; then the staged words' degrees
     u64 scratch64[JN_THREADS / 32 + 1];
-    u32 scratch[JN_THREADS / 32 + 1];
-    LookbackScratch lbs;
+    u32 flags[(JN_TILE / JN_THREADS) * (JN_THREADS / 32)];  // new-word ballots, slot order
+    u32 fbase[(JN_TILE / JN_THREADS) * (JN_THREADS / 32)];
+    u32 nfresh;
     u64 base_cnt, base_deg;
     u32 tile;
 };
@@ -87,13 +88,29 @@ bitmat_step_kernel(CsrSrc<EmitKind::ZV> src, u64 n_probe, const u64 *__restrict_
     const u64 o0 = d0 - i0, o1 = d1 - i1;
     const u64 istart = i0 > 0 ? i0 - 1 : 0;
     const u32 ni = (u32) (i1 - istart);
-    for (u32 j = tid; j < ni; j += JN_THREADS) {
-        const u64 gi = istart + j;
-        u64 begin, payload;
-        src.item(gi, begin, payload);
-        s.obeg[j] = offsets[gi];
-        s.begin[j] = begin;
-        s.payload[j] = (u32) payload;
+    {
+        // rows: probe words and offsets first, then their index entries, so
+        // that a thread's row loads are in flight together
+        constexpr u32 RV = (JN_TILE + 1 + JN_THREADS - 1) / JN_THREADS;
+        const u64 pmask = (1ull << src.bits) - 1;
+        u64 pw[RV];
+#pragma unroll
+        for (u32 r = 0; r < RV; ++r) {
+            const u32 j = tid + r * JN_THREADS;
+            pw[r] = 0;
+            if (j < ni) {
+                pw[r] = src.probe[istart + j];
+                s.obeg[j] = offsets[istart + j];
+            }
+        }
+#pragma unroll
+        for (u32 r = 0; r < RV; ++r) {
+            const u32 j = tid + r * JN_THREADS;
+            if (j < ni) {
+                s.begin[j] = __ldg(src.off + (pw[r] >> src.bits));
+                s.payload[j] = (u32) (pw[r] & pmask);
+            }
+        }
     }
     __syncthreads();
     // phase 1: owner row of every item (shared memory only)
@@ -123,66 +140,97 @@ bitmat_step_kernel(CsrSrc<EmitKind::ZV> src, u64 n_probe, const u64 *__restrict_
     u32 wt[VT];
 #pragma unroll
     for (u32 k = 0; k < VT; ++k) wt[k] = (valid >> k) & 1u ? __ldg(src.val + idx[k]) : 0u;
-    // phase 3: test-and-set
+    // phase 3: test-and-set (all atomics issued before any result is used)
+    u32 old[VT];
+#pragma unroll
+    for (u32 k = 0; k < VT; ++k)
+        old[k] = (valid >> k) & 1u ? atomicOr(&m[(u64) xs[k] * stride + (wt[k] >> 5)], 1u << (wt[k] & 31)) : ~0u;
     u32 fresh = 0;
 #pragma unroll
-    for (u32 k = 0; k < VT; ++k) {
-        if ((valid >> k) & 1u) {
-            const u32 bit = 1u << (wt[k] & 31);
-            const u32 old = atomicOr(&m[(u64) xs[k] * stride + (wt[k] >> 5)], bit);
-            if (!(old & bit)) fresh |= 1u << k;
-        }
-    }
+    for (u32 k = 0; k < VT; ++k)
+        if (!((old[k] >> (wt[k] & 31)) & 1u)) fresh |= 1u << k;
     // phase 4: out-degrees of the new words (their join size next step)
     u32 dg[VT];
-    u64 dsum = 0;
+#pragma unroll
+    for (u32 k = 0; k < VT; ++k) dg[k] = (fresh >> k) & 1u ? __ldg(src.off + wt[k] + 1) - __ldg(src.off + wt[k]) : 0u;
+    // Compaction in join-output order (item k of thread t is slot t + k * JN_THREADS),
+    // so the next delta keeps the probe order: grouped by source x.
+    const u32 lane = tid & 31, warp = tid >> 5;
+    u32 bal[VT];
 #pragma unroll
     for (u32 k = 0; k < VT; ++k) {
-        dg[k] = (fresh >> k) & 1u ? __ldg(src.off + wt[k] + 1) - __ldg(src.off + wt[k]) : 0u;
-        dsum += dg[k];
+        bal[k] = __ballot_sync(0xffffffffu, (fresh >> k) & 1u);
+        if (lane == 0) s.flags[k * (JN_THREADS / 32) + warp] = bal[k];
     }
-    u32 tot_cnt;
-    u32 pos = block_exclusive_sum<JN_THREADS / 32>((u32) __popc(fresh), s.scratch, &tot_cnt);
+    __syncthreads();
+    if (warp == 0) {  // exclusive prefix of the 64 flag words' popcounts, in slot order
+        constexpr u32 NF = VT * (JN_THREADS / 32);
+        static_assert(NF == 64, "two flag words per lane");
+        const u32 c0 = __popc(s.flags[2 * lane]), c1 = __popc(s.flags[2 * lane + 1]);
+        const u32 incl = warp_inclusive_sum(c0 + c1);
+        s.fbase[2 * lane] = incl - c0 - c1;
+        s.fbase[2 * lane + 1] = incl - c1;
+        if (lane == 31) s.nfresh = incl;
+    }
+    __syncthreads();  // rows no longer read: obeg/begin/payload take the staged words
+    const u32 lt = lanemask_lt();
+#pragma unroll
+    for (u32 k = 0; k < VT; ++k) {
+        if ((fresh >> k) & 1u) {
+            const u32 p = s.fbase[k * (JN_THREADS / 32) + warp] + __popc(bal[k] & lt);
+            s.begin[p] = ((u64) wt[k] << src.bits) | xs[k];
+            s.payload[p] = dg[k];
+        }
+    }
+    __syncthreads();
+    const u32 tot_cnt = s.nfresh;
+    // degree prefix over the staged words (blocked: thread t owns VT consecutive)
+    u64 mine = 0;
+#pragma unroll
+    for (u32 k = 0; k < VT; ++k) {
+        const u32 p = tid * VT + k;
+        mine += p < tot_cnt ? s.payload[p] : 0u;
+    }
     u64 tot_deg;
-    u64 dpos = block_exclusive_sum<JN_THREADS / 32>(dsum, s.scratch64, &tot_deg);
-    u64 ec = 0, ed = 0;
+    u64 dpos = block_exclusive_sum<JN_THREADS / 32>(mine, s.scratch64, &tot_deg);
+#pragma unroll
+    for (u32 k = 0; k < VT; ++k) {
+        const u32 p = tid * VT + k;
+        if (p < tot_cnt) {
+            s.obeg[p] = dpos;
+            dpos += s.payload[p];
+        }
+    }
+    // positions in the next delta: look-back on both columns, one warp each
     if (tile == 0) {
         if (tid == 0) {
             st_relaxed_u64(lb_cnt, lb_word(kStatusInc, epoch, tot_cnt));
             st_relaxed_u64(lb_deg, lb_word(kStatusInc, epoch, tot_deg));
+            s.base_cnt = 0;
+            s.base_deg = 0;
         }
     } else {
         if (tid == 0) {
             st_relaxed_u64(lb_cnt + tile, lb_word(kStatusAgg, epoch, tot_cnt));
             st_relaxed_u64(lb_deg + tile, lb_word(kStatusAgg, epoch, tot_deg));
         }
-        ec = lookback_block<JN_THREADS / 32>(lb_cnt, tile, epoch, err, s.lbs);
-        ed = lookback_block<JN_THREADS / 32>(lb_deg, tile, epoch, err, s.lbs);
-        if (tid == 0) {
-            st_relaxed_u64(lb_cnt + tile, lb_word(kStatusInc, epoch, ec + tot_cnt));
-            st_relaxed_u64(lb_deg + tile, lb_word(kStatusInc, epoch, ed + tot_deg));
-        }
-    }
-    if (tid == 0) {
-        s.base_cnt = ec;
-        s.base_deg = ed;
-        if (tile == ntiles - 1) {
-            totals[0] = ec + tot_cnt;
-            totals[1] = ed + tot_deg;
-        }
-    }
-    __syncthreads();  // rows no longer read: obeg/begin take the staged words
-#pragma unroll
-    for (u32 k = 0; k < VT; ++k) {
-        if ((fresh >> k) & 1u) {
-            s.begin[pos] = ((u64) wt[k] << src.bits) | xs[k];
-            s.obeg[pos] = dpos;
-            ++pos;
-            dpos += dg[k];
+        if (warp < 2) {
+            u64 *lb = warp == 0 ? lb_cnt : lb_deg;
+            const u64 mytot = warp == 0 ? (u64) tot_cnt : tot_deg;
+            const u64 ex = lookback_warp(lb, tile, epoch, err);
+            if (lane == 0) {
+                st_relaxed_u64(lb + tile, lb_word(kStatusInc, epoch, ex + mytot));
+                if (warp == 0) s.base_cnt = ex;
+                else s.base_deg = ex;
+            }
         }
     }
     __syncthreads();
     const u64 bc = s.base_cnt, bd = s.base_deg;
+    if (tile == ntiles - 1 && tid == 0) {
+        totals[0] = bc + tot_cnt;
+        totals[1] = bd + tot_deg;
+    }
     for (u32 i = tid; i < tot_cnt; i += JN_THREADS) {
         if (bc + i < capacity) {
             out[bc + i] = s.begin[i];
