@@ -4,20 +4,21 @@
 // subtracting the sorted full relation and merging the difference back in
 // (tc.cu:250-286). Here, when n x n bits fit in device memory (n = distinct
 // node ids; 12.6 GB for 317K nodes), full is a bit matrix M with one row per
-// path source x and one column per path target w, and one semi-naive step is
-// a single pass over the join output: every join word (x, w) sets its bit with
-// atomicOr, and it is a new tuple exactly when the bit was clear before. That
-// is dedup(J) \ full and full u J at once, without materialising J: the
-// delta is the same set as the reference's (each tuple is claimed by exactly
-// one atomic), so per-iteration |delta| and the fixpoint are identical. The
-// result leaves as sorted (target, source) words -- the reference's output
-// order (tc.cu:345-366) -- through a bit-matrix transpose, row popcounts, a
-// scan and an extraction pass.
+// path source x and one column per path target w, and dedup(J) \ full and
+// full u J are one operation: a join tuple (x, w) is new exactly when its bit
+// goes from 0 to 1. The delta is the same set as the reference's (every new
+// bit is claimed by exactly one atomic on M), so per-iteration |delta| and the
+// fixpoint are identical. The result leaves as sorted (target, source) words
+// -- the reference's output order (tc.cu:345-366) -- through a bit-matrix
+// transpose, row popcounts, a scan and an extraction pass.
 //
-// Locality: the first delta is the edge list in source-major order and every
-// later delta is appended tile by tile in probe order, so the probe rows of
-// one source stay close together and its matrix row (n / 8 bytes) stays in L2
-// while their join outputs land in it.
+// A delta is kept as units: one source x and a run of path targets y (u32,
+// at most UNIT_ROWS of them). Almost all join output of a TC iteration
+// belongs to a few heavy (x, iteration) pairs, so a CTA takes a unit, ORs
+// the join words (x, w) for every edge y -> w into a shared-memory copy of
+// row x, and then folds that row into M with one atomicOr per touched word
+// (consecutive words: coalesced), instead of one global atomic per join word.
+// The new bits of the unit are its part of the next delta.
 #include "dl_engine_detail.h"
 #include "dl_join.cuh"
 
@@ -27,217 +28,212 @@ namespace {
 
 constexpr int TR_ROWS = 256;  // source rows per transpose tile
 constexpr int TR_WORDS = 16;  // source words (512 columns) per transpose tile
+constexpr int UT = 512;       // threads of the unit kernel
+constexpr int U_ILP = 4;      // join words per thread in flight
+constexpr u64 UNIT_ROWS = 8192;
 
-// Word (w << bits) | x of a delta -> bit (x, w) of the matrix.
-__global__ void bitmat_set_kernel(const u64 *__restrict__ words, u64 n, int bits, u32 *__restrict__ m, u64 stride) {
+// One source x and delta rows rows[start, start + len): paths x -> rows[i].
+struct Unit {
+    u32 x;
+    u32 len;
+    u64 start;
+};
+
+// Sorted (x << bits) | y edge words -> bit (x, y) of the matrix.
+__global__ void bitmat_set_edges_kernel(const u64 *__restrict__ words, u64 n, int bits, u32 *__restrict__ m,
+                                        u64 stride) {
     const u64 mask = (1ull << bits) - 1;
     for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64) gridDim.x * blockDim.x) {
         const u64 v = words[i];
-        const u64 w = v >> bits, x = v & mask;
-        atomicOr(&m[x * stride + (w >> 5)], 1u << (w & 31));
+        const u64 x = v >> bits, y = v & mask;
+        atomicOr(&m[x * stride + (y >> 5)], 1u << (y & 31));
     }
 }
 
-// Sorted (x << bits) | y edge words -> probe words (y << bits) | x in the
-// same (source-major) order.
-__global__ void swap_fields_kernel(const u64 *__restrict__ in, u64 n, int bits, u64 *__restrict__ out) {
-    const u64 mask = (1ull << bits) - 1;
-    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64) gridDim.x * blockDim.x) {
-        const u64 v = in[i];
-        out[i] = ((v & mask) << bits) | (v >> bits);
+// Units of the first delta (the edges, from the CSR): per[x] = units of x.
+__global__ void units_per_source_kernel(const u32 *__restrict__ off, u64 n, u64 *__restrict__ per) {
+    for (u64 x = (u64) blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (u64) gridDim.x * blockDim.x)
+        per[x] = ((u64) (off[x + 1] - off[x]) + UNIT_ROWS - 1) / UNIT_ROWS;
+}
+
+__global__ void units_fill_kernel(const u32 *__restrict__ off, u64 n, const u64 *__restrict__ first,
+                                  Unit *__restrict__ units) {
+    for (u64 x = (u64) blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (u64) gridDim.x * blockDim.x) {
+        const u64 b = off[x], e = off[x + 1];
+        u64 k = first[x];
+        for (u64 s = b; s < e; s += UNIT_ROWS) units[k++] = Unit{(u32) x, (u32) min(UNIT_ROWS, e - s), s};
     }
 }
 
-struct StepSmem {
-    u64 obeg[JN_TILE + 1];    // first output of each loaded row; then the staged words' next offsets
-    u64 begin[JN_TILE + 1];   // first match of each loaded row; then the staged new words
-    u32 payload[JN_TILE + 1]; // probe value of each loaded row; then the staged words' degrees
-    u64 scratch64[JN_THREADS / 32 + 1];
-    u32 flags[(JN_TILE / JN_THREADS) * (JN_THREADS / 32)];  // new-word ballots, slot order
-    u32 fbase[(JN_TILE / JN_THREADS) * (JN_THREADS / 32)];
-    u32 nfresh;
-    u64 base_cnt, base_deg;
-    u32 tile;
+// sum over edges of the target's out-degree: the first join's size.
+__global__ void edge_degree_sum_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, u64 ne,
+                                       unsigned long long *__restrict__ sum) {
+    u64 s = 0;
+    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += (u64) gridDim.x * blockDim.x) {
+        const u32 y = val[i];
+        s += off[y + 1] - off[y];
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(sum, (unsigned long long) s);
+}
+
+struct UnitSmem {
+    u32 rbeg[UT];        // first edge of each row of the batch
+    u32 rpre[UT + 1];    // exclusive prefix of the rows' degrees
+    u64 scratch64[UT / 32 + 1];
+    u32 scratch[UT / 32 + 1];
+    u32 unit;
+    u32 ndirty;
+    unsigned long long obase;
+    // followed by: u32 row[words]; u16 dirty[words]
 };
 
-// One semi-naive TC step over a delta: for probe row (y << bits) | x and
-// every edge y -> w, test-and-set bit (x, w); the new tuples form the next
-// delta as words (w << bits) | x, in tile order, together with the next
-// step's join offsets (exclusive prefix of the new words' out-degrees) --
-// so the next step needs no count pass. Tiles take their positions in the
-// next delta by decoupled look-back on two columns (new words, their
-// degrees); `totals` gets |next delta| and its join size. The tile/owner
-// layout is the join emit's (rows and outputs merged along a merge path,
-// `splits` from the same partition); the loads and atomics of a thread's
-// items are issued in separate unrolled phases so that they overlap.
-__global__ void __launch_bounds__(JN_THREADS, 4)
-bitmat_step_kernel(CsrSrc<EmitKind::ZV> src, u64 n_probe, const u64 *__restrict__ offsets, u64 total,
-                   const u64 *__restrict__ splits, u32 *__restrict__ m, u64 stride, u64 *__restrict__ out,
-                   u64 *__restrict__ out_offsets, u64 capacity, u64 *lb_cnt, u64 *lb_deg, u32 *tile_ctr, u32 epoch,
-                   u32 ntiles, u32 *err, u64 *totals) {
+// Counters of one step (device, zeroed before the launch).
+struct StepCounters {
+    unsigned long long fetch;   // next unit to take
+    unsigned long long words;   // new tuples (next delta rows)
+    unsigned long long join;    // join size of the next step
+    unsigned long long units;   // units of the next delta
+};
+
+// One semi-naive TC step over the units of a delta (persistent CTAs).
+__global__ void __launch_bounds__(UT, 2)
+bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const u32 *__restrict__ rows,
+                        const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
+                        u32 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap,
+                        StepCounters *__restrict__ ctr, u32 *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StepSmem &s = *reinterpret_cast<StepSmem *>(smem_raw);
-    constexpr u32 VT = JN_TILE / JN_THREADS;
-    const int tid = threadIdx.x;
-    if (tid == 0) s.tile = atomicAdd(tile_ctr, 1u);  // launch order: look-back always progresses
-    __syncthreads();
-    const u32 tile = s.tile;
-    const u64 d0 = (u64) tile * JN_TILE;
-    const u64 d1 = min(d0 + JN_TILE, n_probe + total);
-    const u64 i0 = splits[tile], i1 = splits[tile + 1];
-    const u64 o0 = d0 - i0, o1 = d1 - i1;
-    const u64 istart = i0 > 0 ? i0 - 1 : 0;
-    const u32 ni = (u32) (i1 - istart);
-    {
-        // rows: probe words and offsets first, then their index entries, so
-        // that a thread's row loads are in flight together
-        constexpr u32 RV = (JN_TILE + 1 + JN_THREADS - 1) / JN_THREADS;
-        const u64 pmask = (1ull << src.bits) - 1;
-        u64 pw[RV];
-#pragma unroll
-        for (u32 r = 0; r < RV; ++r) {
-            const u32 j = tid + r * JN_THREADS;
-            pw[r] = 0;
-            if (j < ni) {
-                pw[r] = src.probe[istart + j];
-                s.obeg[j] = offsets[istart + j];
-            }
-        }
-#pragma unroll
-        for (u32 r = 0; r < RV; ++r) {
-            const u32 j = tid + r * JN_THREADS;
-            if (j < ni) {
-                s.begin[j] = __ldg(src.off + (pw[r] >> src.bits));
-                s.payload[j] = (u32) (pw[r] & pmask);
-            }
-        }
-    }
-    __syncthreads();
-    // phase 1: owner row of every item (shared memory only)
-    u64 idx[VT];
-    u32 xs[VT];
-    u32 valid = 0;
-    u32 j = 0;
-#pragma unroll
-    for (u32 k = 0; k < VT; ++k) {
-        idx[k] = 0;
-        xs[k] = 0;
-        const u64 o = o0 + tid + (u64) k * JN_THREADS;
-        if (o < o1) {
-            u32 lo = j, hi = ni;  // last loaded row whose first output is <= o
-            while (lo < hi) {
-                const u32 mid = (lo + hi) >> 1;
-                if (s.obeg[mid] <= o) lo = mid + 1;
-                else hi = mid;
-            }
-            j = lo - 1;
-            idx[k] = s.begin[j] + (o - s.obeg[j]);
-            xs[k] = s.payload[j];
-            valid |= 1u << k;
-        }
-    }
-    // phase 2: edge targets
-    u32 wt[VT];
-#pragma unroll
-    for (u32 k = 0; k < VT; ++k) wt[k] = (valid >> k) & 1u ? __ldg(src.val + idx[k]) : 0u;
-    // phase 3: test-and-set (all atomics issued before any result is used)
-    u32 old[VT];
-#pragma unroll
-    for (u32 k = 0; k < VT; ++k)
-        old[k] = (valid >> k) & 1u ? atomicOr(&m[(u64) xs[k] * stride + (wt[k] >> 5)], 1u << (wt[k] & 31)) : ~0u;
-    u32 fresh = 0;
-#pragma unroll
-    for (u32 k = 0; k < VT; ++k)
-        if (!((old[k] >> (wt[k] & 31)) & 1u)) fresh |= 1u << k;
-    // phase 4: out-degrees of the new words (their join size next step)
-    u32 dg[VT];
-#pragma unroll
-    for (u32 k = 0; k < VT; ++k) dg[k] = (fresh >> k) & 1u ? __ldg(src.off + wt[k] + 1) - __ldg(src.off + wt[k]) : 0u;
-    // Compaction in join-output order (item k of thread t is slot t + k * JN_THREADS),
-    // so the next delta keeps the probe order: grouped by source x.
-    const u32 lane = tid & 31, warp = tid >> 5;
-    u32 bal[VT];
-#pragma unroll
-    for (u32 k = 0; k < VT; ++k) {
-        bal[k] = __ballot_sync(0xffffffffu, (fresh >> k) & 1u);
-        if (lane == 0) s.flags[k * (JN_THREADS / 32) + warp] = bal[k];
-    }
-    __syncthreads();
-    if (warp == 0) {  // exclusive prefix of the 64 flag words' popcounts, in slot order
-        constexpr u32 NF = VT * (JN_THREADS / 32);
-        static_assert(NF == 64, "two flag words per lane");
-        const u32 c0 = __popc(s.flags[2 * lane]), c1 = __popc(s.flags[2 * lane + 1]);
-        const u32 incl = warp_inclusive_sum(c0 + c1);
-        s.fbase[2 * lane] = incl - c0 - c1;
-        s.fbase[2 * lane + 1] = incl - c1;
-        if (lane == 31) s.nfresh = incl;
-    }
-    __syncthreads();  // rows no longer read: obeg/begin/payload take the staged words
+    UnitSmem &s = *reinterpret_cast<UnitSmem *>(smem_raw);
+    u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(UnitSmem));
+    unsigned short *dirty = reinterpret_cast<unsigned short *>(row + words);
+    const u32 tid = threadIdx.x, lane = tid & 31;
     const u32 lt = lanemask_lt();
+    for (u32 k = tid; k < words; k += UT) row[k] = 0;
+    if (tid == 0) s.ndirty = 0;
+    for (;;) {
+        if (tid == 0) s.unit = (u32) min((unsigned long long) nunits, atomicAdd(&ctr->fetch, 1ull));
+        __syncthreads();
+        const u64 ui = s.unit;
+        if (ui >= nunits) break;
+        const Unit U = units[ui];
+        // ---- join words (x, w) of the unit into the shared row ----
+        for (u32 r0 = 0; r0 < U.len; r0 += UT) {
+            const u32 nr = min((u32) UT, U.len - r0);
+            u32 beg = 0, deg = 0;
+            if (tid < nr) {
+                const u32 y = rows[U.start + r0 + tid];
+                beg = __ldg(off + y);
+                deg = __ldg(off + y + 1) - beg;
+            }
+            u32 tot;
+            const u32 pre = block_exclusive_sum<UT / 32>(deg, s.scratch, &tot);
+            s.rbeg[tid] = beg;
+            s.rpre[tid] = pre;
+            __syncthreads();
+            for (u32 i0 = 0; i0 < tot; i0 += UT * U_ILP) {
+                u32 w[U_ILP];
 #pragma unroll
-    for (u32 k = 0; k < VT; ++k) {
-        if ((fresh >> k) & 1u) {
-            const u32 p = s.fbase[k * (JN_THREADS / 32) + warp] + __popc(bal[k] & lt);
-            s.begin[p] = ((u64) wt[k] << src.bits) | xs[k];
-            s.payload[p] = dg[k];
-        }
-    }
-    __syncthreads();
-    const u32 tot_cnt = s.nfresh;
-    // degree prefix over the staged words (blocked: thread t owns VT consecutive)
-    u64 mine = 0;
+                for (int k = 0; k < U_ILP; ++k) {
+                    const u32 i = i0 + k * UT + tid;
+                    w[k] = ~0u;
+                    if (i < tot) {
+                        u32 lo = 0, hi = nr;  // last row whose first output is <= i
+                        while (lo < hi) {
+                            const u32 mid = (lo + hi) >> 1;
+                            if (s.rpre[mid] <= i) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        const u32 j = lo - 1;
+                        w[k] = __ldg(val + s.rbeg[j] + (i - s.rpre[j]));
+                    }
+                }
 #pragma unroll
-    for (u32 k = 0; k < VT; ++k) {
-        const u32 p = tid * VT + k;
-        mine += p < tot_cnt ? s.payload[p] : 0u;
-    }
-    u64 tot_deg;
-    u64 dpos = block_exclusive_sum<JN_THREADS / 32>(mine, s.scratch64, &tot_deg);
+                for (int k = 0; k < U_ILP; ++k) {
+                    bool first = false;
+                    if (w[k] != ~0u) first = atomicOr(&row[w[k] >> 5], 1u << (w[k] & 31)) == 0u;
+                    const u32 b = __ballot_sync(0xffffffffu, first);
+                    if (b) {  // words that became non-zero join the dirty list
+                        u32 base = 0;
+                        if (lane == (u32) (__ffs(b) - 1)) base = atomicAdd(&s.ndirty, (u32) __popc(b));
+                        base = __shfl_sync(0xffffffffu, base, __ffs(b) - 1);
+                        if (first) dirty[base + __popc(b & lt)] = (unsigned short) (w[k] >> 5);
+                    }
+                }
+            }
+            __syncthreads();  // rbeg/rpre free for the next batch
+        }
+        // ---- fold the row into M: new bits = row & ~M ----
+        const u32 nd = s.ndirty;
+        const bool full = (u64) nd * 8 > words;  // many words: walk the row in order (coalesced)
+        const u32 lim = full ? words : nd;
+        const u64 mrow = (u64) U.x * stride;
+        u32 cnt = 0;
+        for (u32 q0 = 0; q0 < lim; q0 += UT * 4) {
+            u32 kk[4], v[4], old[4];
 #pragma unroll
-    for (u32 k = 0; k < VT; ++k) {
-        const u32 p = tid * VT + k;
-        if (p < tot_cnt) {
-            s.obeg[p] = dpos;
-            dpos += s.payload[p];
-        }
-    }
-    // positions in the next delta: look-back on both columns, one warp each
-    if (tile == 0) {
-        if (tid == 0) {
-            st_relaxed_u64(lb_cnt, lb_word(kStatusInc, epoch, tot_cnt));
-            st_relaxed_u64(lb_deg, lb_word(kStatusInc, epoch, tot_deg));
-            s.base_cnt = 0;
-            s.base_deg = 0;
-        }
-    } else {
-        if (tid == 0) {
-            st_relaxed_u64(lb_cnt + tile, lb_word(kStatusAgg, epoch, tot_cnt));
-            st_relaxed_u64(lb_deg + tile, lb_word(kStatusAgg, epoch, tot_deg));
-        }
-        if (warp < 2) {
-            u64 *lb = warp == 0 ? lb_cnt : lb_deg;
-            const u64 mytot = warp == 0 ? (u64) tot_cnt : tot_deg;
-            const u64 ex = lookback_warp(lb, tile, epoch, err);
-            if (lane == 0) {
-                st_relaxed_u64(lb + tile, lb_word(kStatusInc, epoch, ex + mytot));
-                if (warp == 0) s.base_cnt = ex;
-                else s.base_deg = ex;
+            for (int c = 0; c < 4; ++c) {
+                const u32 q = q0 + c * UT + tid;
+                kk[c] = q < lim ? (full ? q : (u32) dirty[q]) : 0u;
+                v[c] = q < lim ? row[kk[c]] : 0u;
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) old[c] = v[c] ? atomicOr(&m[mrow + kk[c]], v[c]) : ~0u;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (v[c]) {
+                    const u32 f = v[c] & ~old[c];
+                    row[kk[c]] = f;
+                    cnt += __popc(f);
+                }
             }
         }
-    }
-    __syncthreads();
-    const u64 bc = s.base_cnt, bd = s.base_deg;
-    if (tile == ntiles - 1 && tid == 0) {
-        totals[0] = bc + tot_cnt;
-        totals[1] = bd + tot_deg;
-    }
-    for (u32 i = tid; i < tot_cnt; i += JN_THREADS) {
-        if (bc + i < capacity) {
-            out[bc + i] = s.begin[i];
-            out_offsets[bc + i] = bd + s.obeg[i];
-        } else {
-            atomicOr(err, DL_DEVERR_CAPACITY);  // more new tuples than join outputs: reported, never written
+        u32 total;
+        u32 pos = block_exclusive_sum<UT / 32>(cnt, s.scratch, &total);
+        if (tid == 0) s.obase = total ? atomicAdd(&ctr->words, (unsigned long long) total) : 0ull;
+        __syncthreads();
+        // ---- emit the new tuples (targets of x), clear the row ----
+        const u64 obase = s.obase;
+        u64 p = obase + pos;
+        u64 dsum = 0;
+        for (u32 q0 = 0; q0 < lim; q0 += UT * 4) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const u32 q = q0 + c * UT + tid;
+                if (q >= lim) continue;
+                const u32 k = full ? q : (u32) dirty[q];
+                u32 f = row[k];
+                if (!f) continue;
+                row[k] = 0;
+                while (f) {
+                    const u32 b = __ffs(f) - 1;
+                    f &= f - 1;
+                    const u32 wv = k * 32 + b;
+                    if (p < out_cap) out[p] = wv;
+                    else atomicOr(err, DL_DEVERR_CAPACITY);  // more new tuples than join words: reported
+                    ++p;
+                    dsum += __ldg(off + wv + 1) - __ldg(off + wv);
+                }
+            }
         }
+        u64 dtot;
+        block_exclusive_sum<UT / 32>(dsum, s.scratch64, &dtot);
+        if (total) {
+            const u64 nsub = (total + UNIT_ROWS - 1) / UNIT_ROWS;
+            if (tid == 0) {
+                if (dtot) atomicAdd(&ctr->join, (unsigned long long) dtot);
+                s.obase = atomicAdd(&ctr->units, (unsigned long long) nsub);
+            }
+            __syncthreads();
+            const u64 ub = s.obase;
+            for (u64 i = tid; i < nsub; i += UT) {
+                if (ub + i < uout_cap)
+                    uout[ub + i] = Unit{U.x, (u32) min(UNIT_ROWS, total - i * UNIT_ROWS), obase + i * UNIT_ROWS};
+                else
+                    atomicOr(err, DL_DEVERR_CAPACITY);
+            }
+        }
+        if (tid == 0) s.ndirty = 0;
+        __syncthreads();
     }
 }
 
@@ -371,76 +367,88 @@ bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n) {
     return need <= ((u64) ctx.tune.bitmap_max_gib << 30) && need <= avail / 2;
 }
 
+
 u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u64 ne, const dl_options &opt,
                        PhaseTimer &pt) {
     Workspace &ws = ctx.ws;
     const u64 n = g.n_ids;
     const u64 stride = bitmat_stride(n);
     const u64 words_used = (n + 31) / 32;
+    const size_t smem = sizeof(UnitSmem) + words_used * 4 + words_used * 2 + 16;
+    if (smem > 227 * 1024) throw Error(DL_ERR_OUT_OF_MEMORY, "bit-matrix rows of " + std::to_string(n) +
+                                                              " nodes do not fit in shared memory");
     DevBuf &M = ws.bitmat[0];
     ctx.reserve(M, std::max<u64>(bitmat_bytes(n), 4));
     DL_CUDA(cudaMemsetAsync(M.p, 0, bitmat_bytes(n), ctx.stream));
     u32 *m = M.as<u32>();
-    // delta_0 = the edges, source-major
-    ctx.reserve(ws.jbuf[0], std::max<u64>(ne, 1) * 8);
-    u64 *delta = ws.jbuf[0].as<u64>();
-    u64 ndelta = ne;
+    StepCounters *ctr = reinterpret_cast<StepCounters *>(&ctx.ctrl->scalar[52]);
+    // delta_0 = the edges: rows are the CSR's values, units from its offsets
+    const u32 *rows = g.csr.val;
+    u64 nunits = 0, join = 0;
+    DevBuf *ubuf = &ws.offsets, *ubuf_next = &ws.offsets_next;
     if (ne) {
-        DL_LAUNCH(ctx, K_PREP, 16.0 * ne,
-                  swap_fields_kernel<<<grid_for(ne, T256, ctx), T256, 0, ctx.stream>>>(edges, ne, g.bits, delta));
         DL_LAUNCH(ctx, K_BITMAP_EXPAND, 16.0 * ne,
-                  bitmat_set_kernel<<<grid_for(ne, T256, ctx), T256, 0, ctx.stream>>>(delta, ne, g.bits, m, stride));
+                  bitmat_set_edges_kernel<<<grid_for(ne, T256, ctx), T256, 0, ctx.stream>>>(edges, ne, g.bits, m,
+                                                                                            stride));
+        ctx.reserve(ws.w0, (n + 1) * 8);
+        ctx.reserve(ws.w1, (n + 1) * 8);
+        DL_LAUNCH(ctx, K_PREP, 12.0 * n,
+                  units_per_source_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n,
+                                                                                           ws.w0.as<u64>()));
+        nunits = exclusive_scan(ctx, ws.w0.as<u64>(), n, ws.w1.as<u64>());
+        ctx.reserve(*ubuf, std::max<u64>(nunits, 1) * sizeof(Unit));
+        DL_LAUNCH(ctx, K_PREP, 16.0 * nunits,
+                  units_fill_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, ws.w1.as<u64>(),
+                                                                                     ubuf->as<Unit>()));
+        DL_CUDA(cudaMemsetAsync(&ctr->join, 0, sizeof(u64), ctx.stream));
+        DL_LAUNCH(ctx, K_PREP, 8.0 * ne,
+                  edge_degree_sum_kernel<<<grid_for(ne, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, g.csr.val, ne,
+                                                                                           &ctr->join));
+        DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, &ctr->join, sizeof(u64), cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        join = ctx.host_scalars[0];
     }
     u64 nfull = ne;
-    // join offsets of delta_0; later deltas get theirs from the step kernel
-    pt.mark(PH_JOIN);
-    ctx.reserve(ws.offsets, std::max<u64>(ndelta, 1) * 8);
-    u64 total = ne ? join_count(ctx, g.csr, delta, ndelta, g.bits, ws.offsets.as<u64>()) : 0;
-    u64 *totals = &ctx.ctrl->scalar[50];
-    const CsrSrc<EmitKind::ZV> src{g.csr.off, g.csr.val, nullptr, g.bits};
-    auto kern = bitmat_step_kernel;
-    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sizeof(StepSmem)));
+    auto kern = bitmat_unit_step_kernel;
+    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int per_sm = 0;
+    DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, UT, smem));
+    const u64 resident = (u64) ctx.sm_count * std::max(per_sm, 1);
+    int slot = 0;
     for (int it = 0; ne > 0; ++it) {  // tc.cu:216-314
         pt.mark(PH_JOIN);
-        ctx.run_join_total += total;
-        ctx.run_join_max = std::max(ctx.run_join_max, total);
-        DevBuf &nbuf = other(ws, delta);
-        ctx.reserve(nbuf, std::max<u64>(total, 1) * 8);
-        ctx.reserve(ws.offsets_next, std::max<u64>(total, 1) * 8);
-        u64 nnew = 0, next_total = 0;
-        if (total) {
+        ctx.run_join_total += join;
+        ctx.run_join_max = std::max(ctx.run_join_max, join);
+        u64 nnew = 0, next_join = 0, next_units = 0;
+        if (join) {
             pt.mark(PH_DEDUP);
-            const u64 tiles = (ndelta + total + JN_TILE - 1) / JN_TILE;
-            ctx.lbs_splits.reserve((tiles + 1) * sizeof(u64));
-            u64 *splits = ctx.lbs_splits.as<u64>();
-            DL_LAUNCH(ctx, K_JOIN_PARTITION, 0,
-                      lbs_partition_kernel<<<(unsigned) ((tiles + 1 + 255) / 256), 256, 0, ctx.stream>>>(
-                          ws.offsets.as<u64>(), ndelta, total, tiles + 1, splits));
-            u64 *lb = ctx.lookback_words(2 * tiles);
-            u32 *ctr = ctx.tile_counter(63);
-            DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(u32), ctx.stream));
-            CsrSrc<EmitKind::ZV> sv = src;
-            sv.probe = delta;
-            DL_LAUNCH(ctx, K_BITMAP_EXPAND, 16.0 * ndelta + 12.0 * total,
-                      kern<<<(unsigned) tiles, JN_THREADS, sizeof(StepSmem), ctx.stream>>>(
-                          sv, ndelta, ws.offsets.as<u64>(), total, splits, m, stride, nbuf.as<u64>(),
-                          ws.offsets_next.as<u64>(), total, lb, lb + tiles, ctr, ctx.next_epoch(), (u32) tiles,
-                          &ctx.ctrl->err, totals));
-            DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, totals, 2 * sizeof(u64), cudaMemcpyDeviceToHost, ctx.stream));
+            DevBuf &obuf = ws.jbuf[slot];
+            ctx.reserve(obuf, join * 4);
+            const u64 ucap = nunits + join / UNIT_ROWS + 1;
+            ctx.reserve(*ubuf_next, ucap * sizeof(Unit));
+            DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(StepCounters), ctx.stream));
+            const unsigned grid = (unsigned) std::min<u64>(nunits, resident);
+            DL_LAUNCH(ctx, K_BITMAP_EXPAND, 4.0 * nunits + 8.0 * join,
+                      kern<<<grid, UT, smem, ctx.stream>>>(g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m,
+                                                           stride, (u32) words_used, obuf.as<u32>(), join,
+                                                           ubuf_next->as<Unit>(), ucap, ctr, &ctx.ctrl->err));
+            DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, ctr, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx.stream));
             ctx.sync();
-            nnew = ctx.host_scalars[0];
-            next_total = ctx.host_scalars[1];
-            ctx.prof_add_bytes(K_BITMAP_EXPAND, 16.0 * nnew);
+            nnew = ctx.host_scalars[1];
+            next_join = ctx.host_scalars[2];
+            next_units = ctx.host_scalars[3];
+            ctx.prof_add_bytes(K_BITMAP_EXPAND, 4.0 * nnew + 16.0 * next_units);
+            rows = obuf.as<u32>();
+            slot ^= 1;
+            std::swap(ubuf, ubuf_next);
         }
         pt.mark(PH_MERGE);
         nfull += nnew;
         r.deltas.push_back((i64) nnew);
-        r.joins.push_back((i64) total);
+        r.joins.push_back((i64) join);
         r.fulls.push_back((i64) nfull);
-        delta = nbuf.as<u64>();
-        ndelta = nnew;
-        total = next_total;
-        std::swap(ws.offsets, ws.offsets_next);
+        nunits = next_units;
+        join = next_join;
         if (nnew == 0) break;  // |full| unchanged
         if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
     }
