@@ -29,7 +29,6 @@ namespace {
 constexpr int TR_ROWS = 256;  // source rows per transpose tile
 constexpr int TR_WORDS = 16;  // source words (512 columns) per transpose tile
 constexpr int UT = 512;       // threads of the unit kernel
-constexpr int U_ILP = 4;      // join words per thread in flight
 constexpr u64 UNIT_ROWS = 8192;
 
 // One source x and delta rows rows[start, start + len): paths x -> rows[i].
@@ -78,12 +77,12 @@ __global__ void edge_degree_sum_kernel(const u32 *__restrict__ off, const u32 *_
 }
 
 struct UnitSmem {
-    u32 rbeg[UT];        // first edge of each row of the batch
-    u32 rpre[UT + 1];    // exclusive prefix of the rows' degrees
+    int wslot[UT / 32][32];  // per-warp window slots
     u64 scratch64[UT / 32 + 1];
     u32 scratch[UT / 32 + 1];
     u32 unit;
     u32 ndirty;
+    u32 next_group;
     unsigned long long obase;
     // followed by: u32 row[words]; u16 dirty[words]
 };
@@ -106,10 +105,13 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
     UnitSmem &s = *reinterpret_cast<UnitSmem *>(smem_raw);
     u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(UnitSmem));
     unsigned short *dirty = reinterpret_cast<unsigned short *>(row + words);
-    const u32 tid = threadIdx.x, lane = tid & 31;
+    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const u32 lt = lanemask_lt();
     for (u32 k = tid; k < words; k += UT) row[k] = 0;
-    if (tid == 0) s.ndirty = 0;
+    if (tid == 0) {
+        s.ndirty = 0;
+        s.next_group = 0;
+    }
     for (;;) {
         if (tid == 0) s.unit = (u32) min((unsigned long long) nunits, atomicAdd(&ctr->fetch, 1ull));
         __syncthreads();
@@ -117,51 +119,60 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
         if (ui >= nunits) break;
         const Unit U = units[ui];
         // ---- join words (x, w) of the unit into the shared row ----
-        for (u32 r0 = 0; r0 < U.len; r0 += UT) {
-            const u32 nr = min((u32) UT, U.len - r0);
+        // Warps take groups of 32 rows; within a group, window t of 32 join
+        // words finds each word's row by a max-scan of the rows starting in
+        // the window (row lanes scatter themselves into a per-warp slot).
+        int *slot = s.wslot[warp];
+        for (;;) {
+            u32 grp = 0;
+            if (lane == 0) grp = atomicAdd(&s.next_group, 1u);
+            grp = __shfl_sync(0xffffffffu, grp, 0);
+            const u32 r0 = grp * 32;
+            if (r0 >= U.len) break;
+            const u32 r = r0 + lane;
             u32 beg = 0, deg = 0;
-            if (tid < nr) {
-                const u32 y = rows[U.start + r0 + tid];
+            if (r < U.len) {
+                const u32 y = rows[U.start + r];
                 beg = __ldg(off + y);
                 deg = __ldg(off + y + 1) - beg;
             }
-            u32 tot;
-            const u32 pre = block_exclusive_sum<UT / 32>(deg, s.scratch, &tot);
-            s.rbeg[tid] = beg;
-            s.rpre[tid] = pre;
-            __syncthreads();
-            for (u32 i0 = 0; i0 < tot; i0 += UT * U_ILP) {
-                u32 w[U_ILP];
+            const u32 incl = warp_inclusive_sum(deg);
+            const u32 pre = incl - deg;
+            const u32 total = __shfl_sync(0xffffffffu, incl, 31);
+            int cur = -1;  // row of the word before the window
+            for (u32 i0 = 0; i0 < total; i0 += 32) {
+                slot[lane] = -1;
+                __syncwarp();
+                if (deg && pre >= i0 && pre < i0 + 32) slot[pre - i0] = (int) lane;
+                __syncwarp();
+                int o = slot[lane];
 #pragma unroll
-                for (int k = 0; k < U_ILP; ++k) {
-                    const u32 i = i0 + k * UT + tid;
-                    w[k] = ~0u;
-                    if (i < tot) {
-                        u32 lo = 0, hi = nr;  // last row whose first output is <= i
-                        while (lo < hi) {
-                            const u32 mid = (lo + hi) >> 1;
-                            if (s.rpre[mid] <= i) lo = mid + 1;
-                            else hi = mid;
-                        }
-                        const u32 j = lo - 1;
-                        w[k] = __ldg(val + s.rbeg[j] + (i - s.rpre[j]));
-                    }
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, o, d);
+                    if (lane >= (u32) d) o = max(o, t);
                 }
-#pragma unroll
-                for (int k = 0; k < U_ILP; ++k) {
-                    bool first = false;
-                    if (w[k] != ~0u) first = atomicOr(&row[w[k] >> 5], 1u << (w[k] & 31)) == 0u;
-                    const u32 b = __ballot_sync(0xffffffffu, first);
-                    if (b) {  // words that became non-zero join the dirty list
-                        u32 base = 0;
-                        if (lane == (u32) (__ffs(b) - 1)) base = atomicAdd(&s.ndirty, (u32) __popc(b));
-                        base = __shfl_sync(0xffffffffu, base, __ffs(b) - 1);
-                        if (first) dirty[base + __popc(b & lt)] = (unsigned short) (w[k] >> 5);
-                    }
+                o = max(o, cur);
+                cur = __shfl_sync(0xffffffffu, o, 31);
+                const u32 ob = __shfl_sync(0xffffffffu, beg, o);
+                const u32 op = __shfl_sync(0xffffffffu, pre, o);
+                const u32 i = i0 + lane;
+                u32 w = 0;
+                bool first = false;
+                if (i < total) {
+                    w = __ldg(val + ob + (i - op));
+                    first = atomicOr(&row[w >> 5], 1u << (w & 31)) == 0u;
                 }
+                const u32 b = __ballot_sync(0xffffffffu, first);
+                if (b) {  // words that became non-zero join the dirty list
+                    u32 base = 0;
+                    if (lane == (u32) (__ffs(b) - 1)) base = atomicAdd(&s.ndirty, (u32) __popc(b));
+                    base = __shfl_sync(0xffffffffu, base, __ffs(b) - 1);
+                    if (first) dirty[base + __popc(b & lt)] = (unsigned short) (w >> 5);
+                }
+                __syncwarp();  // slot reads done before the next window resets it
             }
-            __syncthreads();  // rbeg/rpre free for the next batch
         }
+        __syncthreads();
         // ---- fold the row into M: new bits = row & ~M ----
         const u32 nd = s.ndirty;
         const bool full = (u64) nd * 8 > words;  // many words: walk the row in order (coalesced)
@@ -232,7 +243,10 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                     atomicOr(err, DL_DEVERR_CAPACITY);
             }
         }
-        if (tid == 0) s.ndirty = 0;
+        if (tid == 0) {
+            s.ndirty = 0;
+            s.next_group = 0;
+        }
         __syncthreads();
     }
 }
