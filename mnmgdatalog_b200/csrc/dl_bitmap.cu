@@ -26,7 +26,7 @@ namespace dl {
 namespace detail {
 namespace {
 
-constexpr int TR_ROWS = 256;  // source rows per transpose tile
+constexpr int TR_ROWS = 512;  // source rows per transpose tile
 constexpr int TR_WORDS = 16;  // source words (512 columns) per transpose tile
 constexpr int UT = 512;       // threads of the unit kernel
 constexpr u64 UNIT_ROWS = 8192;
@@ -266,26 +266,29 @@ __device__ __forceinline__ u32 transpose32(u32 v, u32 lane) {
     return v;
 }
 
-// t = transpose of a (both n rows of `stride` words). A tile is 256 source
-// rows x 512 columns; the 512 target rows each receive 8 words (32 bytes).
-__global__ void __launch_bounds__(256) bitmat_transpose_kernel(const u32 *__restrict__ a, u32 *__restrict__ t, u64 n,
-                                                               u64 stride) {
-    __shared__ u32 in[TR_ROWS][TR_WORDS + 1];
-    __shared__ u32 outw[TR_WORDS * 32][TR_ROWS / 32 + 1];
+// t = transpose of a (both n rows of `stride` words). A tile is 512 source
+// rows x 512 columns: 64 bytes read from every source row and 64 bytes
+// written to every target row. One warp per 32 source rows.
+constexpr int TR_SMEM = 2 * TR_ROWS * (TR_WORDS + 1) * 4;
+__global__ void __launch_bounds__(TR_ROWS) bitmat_transpose_kernel(const u32 *__restrict__ a, u32 *__restrict__ t,
+                                                                   u64 n, u64 stride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    u32(*in)[TR_WORDS + 1] = reinterpret_cast<u32(*)[TR_WORDS + 1]>(smem_raw);
+    u32(*outw)[TR_ROWS / 32 + 1] = reinterpret_cast<u32(*)[TR_ROWS / 32 + 1]>(smem_raw + TR_ROWS * (TR_WORDS + 1) * 4);
+    static_assert(TR_WORDS * 32 == TR_ROWS && TR_ROWS / 32 == TR_WORDS, "square tile: 512 x 512 bits");
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const u64 x0 = (u64) blockIdx.y * TR_ROWS;
     const u64 c0 = (u64) blockIdx.x * TR_WORDS;
-    for (u32 i = tid; i < TR_ROWS * TR_WORDS; i += 256) {
+    for (u32 i = tid; i < TR_ROWS * TR_WORDS; i += TR_ROWS) {
         const u32 r = i / TR_WORDS, c = i % TR_WORDS;
         const u64 x = x0 + r, col = c0 + c;
-        in[r][c] = (x < n && col < stride) ? a[x * stride + col] : 0u;
+        in[r][c] = (x < n && col < stride) ? __ldcs(a + x * stride + col) : 0u;
     }
     __syncthreads();
-    // warp w transposes source rows w*32 .. w*32+31 (target word w of the tile)
 #pragma unroll 4
     for (u32 c = 0; c < TR_WORDS; ++c) outw[c * 32 + lane][warp] = transpose32(in[warp * 32 + lane][c], lane);
     __syncthreads();
-    for (u32 i = tid; i < TR_WORDS * 32 * (TR_ROWS / 32); i += 256) {
+    for (u32 i = tid; i < TR_WORDS * 32 * (TR_ROWS / 32); i += TR_ROWS) {
         const u32 r = i / (TR_ROWS / 32), xw = i % (TR_ROWS / 32);
         const u64 w = c0 * 32 + r, col = x0 / 32 + xw;
         if (w < n && col < stride) t[w * stride + col] = outw[r][xw];
@@ -306,32 +309,47 @@ __global__ void bitmat_row_count_kernel(const u32 *__restrict__ t, u64 n, u64 st
 }
 
 // Row w of t -> words (w << bits) | x for its set bits x, ascending, from
-// out[first[w]] on (warp per row).
-__global__ void bitmat_extract_kernel(const u32 *__restrict__ t, u64 n, u64 stride, u64 words, int bits,
-                                      const u64 *__restrict__ first, u64 *__restrict__ out) {
-    const u32 lane = threadIdx.x & 31;
-    const u64 warps = (u64) gridDim.x * (blockDim.x / 32);
-    for (u64 w = ((u64) blockIdx.x * blockDim.x + threadIdx.x) / 32; w < n; w += warps) {
+// out[first[w]] on (warp per row). A lane takes 4 consecutive words per step
+// (one 16-byte load); a step's words are staged in shared memory and leave
+// with consecutive stores unless there are more than EX_STAGE of them.
+constexpr int EX_THREADS = 256;
+constexpr int EX_STAGE = 256;
+__global__ void __launch_bounds__(EX_THREADS) bitmat_extract_kernel(const u32 *__restrict__ t, u64 n, u64 stride,
+                                                                    u64 words, int bits, const u64 *__restrict__ first,
+                                                                    u64 *__restrict__ out) {
+    __shared__ u64 stage[EX_THREADS / 32][EX_STAGE];
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u64 *st = stage[warp];
+    const u64 warps = (u64) gridDim.x * (EX_THREADS / 32);
+    for (u64 w = (u64) blockIdx.x * (EX_THREADS / 32) + warp; w < n; w += warps) {
         const u32 *row = t + w * stride;
         u64 pos = first[w];
         const u64 hi = w << bits;
-        for (u64 k0 = 0; k0 < words; k0 += 32) {
-            const u64 k = k0 + lane;
-            u32 v = k < words ? __ldcs(row + k) : 0u;
-            const u32 c = __popc(v);
-            // exclusive prefix of the lanes' counts
-            u32 incl = c;
+        for (u64 k0 = 0; k0 < words; k0 += 128) {
+            const u64 k = k0 + lane * 4;  // stride is a multiple of 32 words: the vector stays in the row
+            uint4 q = make_uint4(0, 0, 0, 0);
+            if (k < words) q = __ldcs(reinterpret_cast<const uint4 *>(row + k));
+            u32 v[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const u32 y = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= (u32) d) incl += y;
-            }
+            for (int c = 0; c < 4; ++c)
+                if (k + c >= words) v[c] = 0;  // past the used columns
+            const u32 cnt = __popc(v[0]) + __popc(v[1]) + __popc(v[2]) + __popc(v[3]);
+            const u32 incl = warp_inclusive_sum(cnt);
             const u32 sum = __shfl_sync(0xffffffffu, incl, 31);
-            u64 p = pos + (incl - c);
-            while (v) {
-                const int b = __ffs(v) - 1;
-                v &= v - 1;
-                out[p++] = hi | (k * 32 + (u64) b);
+            if (sum == 0) continue;
+            u32 p = incl - cnt;
+            if (sum <= EX_STAGE) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    for (u32 b = v[c]; b; b &= b - 1) st[p++] = hi | ((k + c) * 32 + (u64) (__ffs(b) - 1));
+                __syncwarp();
+                for (u32 i = lane; i < sum; i += 32) out[pos + i] = st[i];
+                __syncwarp();
+            } else {
+                u64 q2 = pos + p;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    for (u32 b = v[c]; b; b &= b - 1) out[q2++] = hi | ((k + c) * 32 + (u64) (__ffs(b) - 1));
             }
             pos += sum;
         }
@@ -473,8 +491,9 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         DevBuf &T = ws.bitmat[1];
         ctx.reserve(T, bitmat_bytes(n));
         const dim3 tg((unsigned) (stride / TR_WORDS), (unsigned) ((n + TR_ROWS - 1) / TR_ROWS));
+        DL_CUDA(cudaFuncSetAttribute(bitmat_transpose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TR_SMEM));
         DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 2.0 * bitmat_bytes(n),
-                  bitmat_transpose_kernel<<<tg, 256, 0, ctx.stream>>>(m, T.as<u32>(), n, stride));
+                  bitmat_transpose_kernel<<<tg, TR_ROWS, TR_SMEM, ctx.stream>>>(m, T.as<u32>(), n, stride));
         ctx.reserve(ws.offsets, (n + 1) * 8);
         u64 *counts = ws.offsets.as<u64>();
         ctx.reserve(ws.w0, (n + 1) * 8);
@@ -487,8 +506,8 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
             throw Error(DL_ERR_INTERNAL, "bit matrix holds " + std::to_string(total) + " tuples, expected " +
                                              std::to_string(nfull));
         DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 4.0 * n * words_used + 8.0 * nfull,
-                  bitmat_extract_kernel<<<rg, T256, 0, ctx.stream>>>(T.as<u32>(), n, stride, words_used, g.bits, first,
-                                                                     ws.full[0].as<u64>()));
+                  bitmat_extract_kernel<<<grid_for(n * 32, EX_THREADS, ctx, 8), EX_THREADS, 0, ctx.stream>>>(
+                      T.as<u32>(), n, stride, words_used, g.bits, first, ws.full[0].as<u64>()));
     }
     return nfull;
 }
