@@ -81,10 +81,9 @@ struct UnitSmem {
     u64 scratch64[UT / 32 + 1];
     u32 scratch[UT / 32 + 1];
     u32 unit;
-    u32 ndirty;
     u32 next_group;
     unsigned long long obase;
-    // followed by: u32 row[words]; u16 dirty[words]
+    // followed by: u32 row[words]
 };
 
 // Counters of one step (device, zeroed before the launch).
@@ -96,7 +95,7 @@ struct StepCounters {
 };
 
 // One semi-naive TC step over the units of a delta (persistent CTAs).
-__global__ void __launch_bounds__(UT, 2)
+__global__ void __launch_bounds__(UT, 4)
 bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const u32 *__restrict__ rows,
                         const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
                         u32 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap,
@@ -104,14 +103,9 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
     extern __shared__ __align__(16) unsigned char smem_raw[];
     UnitSmem &s = *reinterpret_cast<UnitSmem *>(smem_raw);
     u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(UnitSmem));
-    unsigned short *dirty = reinterpret_cast<unsigned short *>(row + words);
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const u32 lt = lanemask_lt();
     for (u32 k = tid; k < words; k += UT) row[k] = 0;
-    if (tid == 0) {
-        s.ndirty = 0;
-        s.next_group = 0;
-    }
+    if (tid == 0) s.next_group = 0;
     for (;;) {
         if (tid == 0) s.unit = (u32) min((unsigned long long) nunits, atomicAdd(&ctr->fetch, 1ull));
         __syncthreads();
@@ -119,9 +113,10 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
         if (ui >= nunits) break;
         const Unit U = units[ui];
         // ---- join words (x, w) of the unit into the shared row ----
-        // Warps take groups of 32 rows; within a group, window t of 32 join
-        // words finds each word's row by a max-scan of the rows starting in
-        // the window (row lanes scatter themselves into a per-warp slot).
+        // Warps take groups of 32 rows. A row with 32 or more edges is walked
+        // by the whole warp; for the others, each window of 32 join words
+        // finds every word's row by a max-scan of the rows starting in the
+        // window (row lanes scatter themselves into a per-warp slot).
         int *slot = s.wslot[warp];
         for (;;) {
             u32 grp = 0;
@@ -136,6 +131,24 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                 beg = __ldg(off + y);
                 deg = __ldg(off + y + 1) - beg;
             }
+            // rows with 32 or more edges: the whole warp walks the edge list
+            for (u32 big = __ballot_sync(0xffffffffu, deg >= 32); big; big &= big - 1) {
+                const u32 j = __ffs(big) - 1;
+                const u32 b0 = __shfl_sync(0xffffffffu, beg, j), d0 = __shfl_sync(0xffffffffu, deg, j);
+                for (u32 i0 = 0; i0 < d0; i0 += 32 * 4) {
+                    u32 wv[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const u32 i = i0 + c * 32 + lane;
+                        wv[c] = i < d0 ? __ldg(val + b0 + i) : ~0u;
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (wv[c] != ~0u) atomicOr(&row[wv[c] >> 5], 1u << (wv[c] & 31));
+                }
+            }
+            // the other rows: windows of 32 join words
+            if (deg >= 32) deg = 0;
             const u32 incl = warp_inclusive_sum(deg);
             const u32 pre = incl - deg;
             const u32 total = __shfl_sync(0xffffffffu, incl, 31);
@@ -156,27 +169,16 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                 const u32 ob = __shfl_sync(0xffffffffu, beg, o);
                 const u32 op = __shfl_sync(0xffffffffu, pre, o);
                 const u32 i = i0 + lane;
-                u32 w = 0;
-                bool first = false;
                 if (i < total) {
-                    w = __ldg(val + ob + (i - op));
-                    first = atomicOr(&row[w >> 5], 1u << (w & 31)) == 0u;
-                }
-                const u32 b = __ballot_sync(0xffffffffu, first);
-                if (b) {  // words that became non-zero join the dirty list
-                    u32 base = 0;
-                    if (lane == (u32) (__ffs(b) - 1)) base = atomicAdd(&s.ndirty, (u32) __popc(b));
-                    base = __shfl_sync(0xffffffffu, base, __ffs(b) - 1);
-                    if (first) dirty[base + __popc(b & lt)] = (unsigned short) (w >> 5);
+                    const u32 w = __ldg(val + ob + (i - op));
+                    atomicOr(&row[w >> 5], 1u << (w & 31));
                 }
                 __syncwarp();  // slot reads done before the next window resets it
             }
         }
         __syncthreads();
         // ---- fold the row into M: new bits = row & ~M ----
-        const u32 nd = s.ndirty;
-        const bool full = (u64) nd * 8 > words;  // many words: walk the row in order (coalesced)
-        const u32 lim = full ? words : nd;
+        const u32 lim = words;  // the whole row, in order: coalesced atomics on M
         const u64 mrow = (u64) U.x * stride;
         u32 cnt = 0;
         for (u32 q0 = 0; q0 < lim; q0 += UT * 4) {
@@ -184,7 +186,7 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const u32 q = q0 + c * UT + tid;
-                kk[c] = q < lim ? (full ? q : (u32) dirty[q]) : 0u;
+                kk[c] = q;
                 v[c] = q < lim ? row[kk[c]] : 0u;
             }
 #pragma unroll
@@ -211,7 +213,7 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
             for (int c = 0; c < 4; ++c) {
                 const u32 q = q0 + c * UT + tid;
                 if (q >= lim) continue;
-                const u32 k = full ? q : (u32) dirty[q];
+                const u32 k = q;
                 u32 f = row[k];
                 if (!f) continue;
                 row[k] = 0;
@@ -243,10 +245,7 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                     atomicOr(err, DL_DEVERR_CAPACITY);
             }
         }
-        if (tid == 0) {
-            s.ndirty = 0;
-            s.next_group = 0;
-        }
+        if (tid == 0) s.next_group = 0;
         __syncthreads();
     }
 }
@@ -406,7 +405,7 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
     const u64 n = g.n_ids;
     const u64 stride = bitmat_stride(n);
     const u64 words_used = (n + 31) / 32;
-    const size_t smem = sizeof(UnitSmem) + words_used * 4 + words_used * 2 + 16;
+    const size_t smem = sizeof(UnitSmem) + words_used * 4 + 16;
     if (smem > 227 * 1024) throw Error(DL_ERR_OUT_OF_MEMORY, "bit-matrix rows of " + std::to_string(n) +
                                                               " nodes do not fit in shared memory");
     DevBuf &M = ws.bitmat[0];
