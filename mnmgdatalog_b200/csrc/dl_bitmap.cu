@@ -77,7 +77,8 @@ __global__ void edge_degree_sum_kernel(const u32 *__restrict__ off, const u32 *_
 }
 
 struct UnitSmem {
-    int wslot[UT / 32][32];  // per-warp window slots
+    u32 wbeg[UT / 32][32];   // per-warp compacted rows: first edge
+    u32 wdeg[UT / 32][32];   // and degree
     u64 scratch64[UT / 32 + 1];
     u32 scratch[UT / 32 + 1];
     u32 unit;
@@ -104,6 +105,7 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
     UnitSmem &s = *reinterpret_cast<UnitSmem *>(smem_raw);
     u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(UnitSmem));
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u32 lt = lanemask_lt();
     for (u32 k = tid; k < words; k += UT) row[k] = 0;
     if (tid == 0) s.next_group = 0;
     for (;;) {
@@ -114,10 +116,7 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
         const Unit U = units[ui];
         // ---- join words (x, w) of the unit into the shared row ----
         // Warps take groups of 32 rows. A row with 32 or more edges is walked
-        // by the whole warp; for the others, each window of 32 join words
-        // finds every word's row by a max-scan of the rows starting in the
-        // window (row lanes scatter themselves into a per-warp slot).
-        int *slot = s.wslot[warp];
+        // by the whole warp; the others are expanded 32 join words at a time.
         for (;;) {
             u32 grp = 0;
             if (lane == 0) grp = atomicAdd(&s.next_group, 1u);
@@ -147,33 +146,40 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                         if (wv[c] != ~0u) atomicOr(&row[wv[c] >> 5], 1u << (wv[c] & 31));
                 }
             }
-            // the other rows: windows of 32 join words
+            // the other non-empty rows, compacted to the low lanes: windows of
+            // 32 join words; the rows starting in a window are a bit mask, and
+            // a word's row is the number of rows started up to its position
             if (deg >= 32) deg = 0;
-            const u32 incl = warp_inclusive_sum(deg);
-            const u32 pre = incl - deg;
-            const u32 total = __shfl_sync(0xffffffffu, incl, 31);
-            int cur = -1;  // row of the word before the window
-            for (u32 i0 = 0; i0 < total; i0 += 32) {
-                slot[lane] = -1;
-                __syncwarp();
-                if (deg && pre >= i0 && pre < i0 + 32) slot[pre - i0] = (int) lane;
-                __syncwarp();
-                int o = slot[lane];
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, o, d);
-                    if (lane >= (u32) d) o = max(o, t);
+            const u32 nz = __ballot_sync(0xffffffffu, deg != 0);
+            if (nz) {
+                if (deg) {
+                    const u32 rk = __popc(nz & lt);
+                    s.wbeg[warp][rk] = beg;
+                    s.wdeg[warp][rk] = deg;
                 }
-                o = max(o, cur);
-                cur = __shfl_sync(0xffffffffu, o, 31);
-                const u32 ob = __shfl_sync(0xffffffffu, beg, o);
-                const u32 op = __shfl_sync(0xffffffffu, pre, o);
-                const u32 i = i0 + lane;
-                if (i < total) {
-                    const u32 w = __ldg(val + ob + (i - op));
-                    atomicOr(&row[w >> 5], 1u << (w & 31));
+                __syncwarp();
+                const u32 nrows = __popc(nz);
+                beg = lane < nrows ? s.wbeg[warp][lane] : 0u;
+                deg = lane < nrows ? s.wdeg[warp][lane] : 0u;
+                __syncwarp();
+                const u32 incl = warp_inclusive_sum(deg);
+                const u32 pre = incl - deg;
+                const u32 total = __shfl_sync(0xffffffffu, incl, 31);
+                const u32 le = lane == 31 ? ~0u : (2u << lane) - 1;  // positions <= lane
+                int base = -1;  // last row started before the window
+                for (u32 i0 = 0; i0 < total; i0 += 32) {
+                    const u32 st = (deg && pre >= i0 && pre < i0 + 32) ? 1u << (pre - i0) : 0u;
+                    const u32 starts = __reduce_or_sync(0xffffffffu, st);
+                    const int o = base + __popc(starts & le);
+                    base += __popc(starts);
+                    const u32 ob = __shfl_sync(0xffffffffu, beg, o);
+                    const u32 op = __shfl_sync(0xffffffffu, pre, o);
+                    const u32 i = i0 + lane;
+                    if (i < total) {
+                        const u32 w = __ldg(val + ob + (i - op));
+                        atomicOr(&row[w >> 5], 1u << (w & 31));
+                    }
                 }
-                __syncwarp();  // slot reads done before the next window resets it
             }
         }
         __syncthreads();
