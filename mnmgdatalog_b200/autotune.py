@@ -5,8 +5,9 @@
 Times candidate settings on a sample workload -- the radix pass variant
 (three-kernel LSD or onesweep, shared-memory or ballot ranking, onesweep
 tile), the dense/sparse threshold and the small-run fold threshold of the
-semi-naive step, and the default load factor of the C-ABI hash table (on a
-join of the sample's edges) -- by coordinate descent, keeps the fastest, and
+semi-naive step, for TC the bit-matrix dedup against the tuned sort path,
+and the default load factor of the C-ABI hash table (on a join of the
+sample's edges) -- by coordinate descent, keeps the fastest, and
 checks that every candidate gives identical results (iterations,
 per-iteration deltas, rows). The knobs never change results, only time.
 autotune_batch() does the same for the batched form (dl_run_batch of a sample
@@ -26,6 +27,7 @@ SORT_VARIANTS = [  # (sort_algorithm, sort_ranking, sort_keys_per_thread, sort_i
 ]
 RATIOS = [2, 4, 8]
 LOAD_FACTORS = [0.25, 0.5, 0.7]
+BITMAP_GIB = [48, 0]  # TC dedup: bit matrix when it fits in 48 GiB, or never (sort path)
 
 
 def candidates(stage: str, best: dict) -> list[dict]:
@@ -41,6 +43,8 @@ def candidates(stage: str, best: dict) -> list[dict]:
         out = [dict(best, small_ratio=v) for v in RATIOS]
     elif stage == "hash_load_factor":
         out = [dict(best, hash_load_factor=v) for v in LOAD_FACTORS]
+    elif stage == "bitmap_max_gib":
+        out = [dict(best, bitmap_max_gib=v) for v in BITMAP_GIB]
     else:
         raise ValueError(stage)
     uniq = []
@@ -113,7 +117,9 @@ def autotune(eng, program: str, edges, *, repeats: int = 2, log=print) -> dict:
                int((rows[:, 0] * 1000003 + rows[:, 1]).sum().item()) if len(rows) else 0)
         return r.seconds, sig
 
-    res = tune(eng, run, repeats=repeats, log=log)
+    # TC: the sort path's knobs first, then bit matrix against the tuned sort path
+    stages = ("sort", "dense_ratio", "small_ratio") + (("bitmap_max_gib",) if program == "tc" else ())
+    res = tune(eng, run, stages=stages, repeats=repeats, log=log)
     res2 = tune(eng, _join_workload(d_edges.contiguous()), stages=("hash_load_factor",), repeats=repeats, log=log)
     return {"tuning": res2["tuning"], "trials": res["trials"] + res2["trials"]}
 

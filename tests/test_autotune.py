@@ -15,7 +15,7 @@ def test_sort_stage_covers_every_variant_once():
 
 def test_ratio_and_load_factor_stages_vary_one_knob():
     for stage, values in (("dense_ratio", autotune.RATIOS), ("small_ratio", autotune.RATIOS),
-                          ("hash_load_factor", autotune.LOAD_FACTORS)):
+                          ("hash_load_factor", autotune.LOAD_FACTORS), ("bitmap_max_gib", autotune.BITMAP_GIB)):
         c = autotune.candidates(stage, BASE)
         assert [x[stage] for x in c] == values
         for x in c:

@@ -56,7 +56,7 @@ def test_autotune_small_sample(tmp_path):
         res = autotune.autotune(eng, "tc", edges, repeats=1, log=lambda *_: None)
         assert eng.tuning() == res["tuning"]
         stages = {t["stage"] for t in res["trials"]}
-        assert stages == {"sort", "dense_ratio", "small_ratio", "hash_load_factor"}
+        assert stages == {"sort", "dense_ratio", "small_ratio", "bitmap_max_gib", "hash_load_factor"}
         plain = eng.tc(edges)
     with Engine(0) as ref:
         want = ref.tc(edges)
