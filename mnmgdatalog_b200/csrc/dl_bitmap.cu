@@ -284,10 +284,17 @@ __global__ void __launch_bounds__(TR_ROWS) bitmat_transpose_kernel(const u32 *__
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const u64 x0 = (u64) blockIdx.y * TR_ROWS;
     const u64 c0 = (u64) blockIdx.x * TR_WORDS;
-    for (u32 i = tid; i < TR_ROWS * TR_WORDS; i += TR_ROWS) {
-        const u32 r = i / TR_WORDS, c = i % TR_WORDS;
+    u32 v[TR_WORDS];  // all of a thread's loads in flight before the first store
+#pragma unroll
+    for (u32 j = 0; j < TR_WORDS; ++j) {
+        const u32 i = tid + j * TR_ROWS, r = i / TR_WORDS, c = i % TR_WORDS;
         const u64 x = x0 + r, col = c0 + c;
-        in[r][c] = (x < n && col < stride) ? __ldcs(a + x * stride + col) : 0u;
+        v[j] = (x < n && col < stride) ? __ldcs(a + x * stride + col) : 0u;
+    }
+#pragma unroll
+    for (u32 j = 0; j < TR_WORDS; ++j) {
+        const u32 i = tid + j * TR_ROWS;
+        in[i / TR_WORDS][i % TR_WORDS] = v[j];
     }
     __syncthreads();
 #pragma unroll 4
@@ -446,6 +453,7 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         join = ctx.host_scalars[0];
     }
     u64 nfull = ne;
+    u64 nrows = ne;  // rows of the current delta
     auto kern = bitmat_unit_step_kernel;
     DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int per_sm = 0;
@@ -465,7 +473,8 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
             ctx.reserve(*ubuf_next, ucap * sizeof(Unit));
             DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(StepCounters), ctx.stream));
             const unsigned grid = (unsigned) std::min<u64>(nunits, resident);
-            DL_LAUNCH(ctx, K_BITMAP_EXPAND, 4.0 * nunits + 8.0 * join,
+            // algorithmic bytes: delta rows and units in, one edge target per join word, new rows and units out
+            DL_LAUNCH(ctx, K_BITMAP_EXPAND, 4.0 * nrows + 16.0 * nunits + 4.0 * join,
                       kern<<<grid, UT, smem, ctx.stream>>>(g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m,
                                                            stride, (u32) words_used, obuf.as<u32>(), join,
                                                            ubuf_next->as<Unit>(), ucap, ctr, &ctx.ctrl->err));
@@ -476,6 +485,7 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
             next_units = ctx.host_scalars[3];
             ctx.prof_add_bytes(K_BITMAP_EXPAND, 4.0 * nnew + 16.0 * next_units);
             rows = obuf.as<u32>();
+            nrows = nnew;
             slot ^= 1;
             std::swap(ubuf, ubuf_next);
         }

@@ -75,8 +75,8 @@ enum KernelId : int {
     K_HASH_BUILD,      // C-ABI hash table insert / value extraction
     K_SPARSE_DIFF,     // sparse set difference probes (+ run sampling)
     K_HASH_INSERT,     // hash-set dedup: 8 B read + 32 B probe sector per word, 40 B per new word
-    K_BITMAP_EXPAND,   // bit-matrix TC step: 8 B per delta row + 4 B edge value + 8 B bit-word update per
-                       // join word + 8 B per new word
+    K_BITMAP_EXPAND,   // bit-matrix TC step: 4 B per delta row in and out + 16 B per unit in and out +
+                       // 4 B edge target per join word
     K_BITMAP_EXTRACT,  // bit-matrix transpose, row counts, scan and word extraction of the result
     // host-side costs, counted with or without profiling (seconds = host wall time)
     K_HOST_MALLOC,     // cudaMalloc of a buffer that had to grow (bytes = size)

@@ -30,7 +30,7 @@ CLASSES = [
     (r"join_emit_kernel|join_emit_bucket_kernel", "join_emit"),
     (r"digit0_hist_kernel", "join_count_scan"),
     (r"bucket_starts_kernel", "join_partition"),
-    (r"bitmat_expand_kernel|bitmat_set_kernel", "bitmap_expand"),
+    (r"bitmat_unit_step_kernel|bitmat_set_edges_kernel", "bitmap_expand"),
     (r"bitmat_transpose_kernel|bitmat_row_count_kernel|bitmat_extract_kernel|scan_kernel<.*CountValue",
      "bitmap_extract"),
     (r"lbs_partition_kernel", "join_partition"),
