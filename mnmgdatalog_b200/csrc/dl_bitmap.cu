@@ -29,7 +29,7 @@ namespace {
 constexpr int TR_ROWS = 512;  // source rows per transpose tile
 constexpr int TR_WORDS = 16;  // source words (512 columns) per transpose tile
 constexpr int UT = 512;       // threads of the unit kernel
-constexpr u64 UNIT_ROWS = 8192;
+constexpr u64 UNIT_ROWS = 65536;  // fewer, larger units: each costs a fold of the whole row
 
 // One source x and delta rows rows[start, start + len): paths x -> rows[i].
 struct Unit {
@@ -115,8 +115,7 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
         if (ui >= nunits) break;
         const Unit U = units[ui];
         // ---- join words (x, w) of the unit into the shared row ----
-        // Warps take groups of 32 rows. A row with 32 or more edges is walked
-        // by the whole warp; the others are expanded 32 join words at a time.
+        // Warps take groups of 32 rows and expand them 32 join words at a time.
         for (;;) {
             u32 grp = 0;
             if (lane == 0) grp = atomicAdd(&s.next_group, 1u);
@@ -130,26 +129,9 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                 beg = __ldg(off + y);
                 deg = __ldg(off + y + 1) - beg;
             }
-            // rows with 32 or more edges: the whole warp walks the edge list
-            for (u32 big = __ballot_sync(0xffffffffu, deg >= 32); big; big &= big - 1) {
-                const u32 j = __ffs(big) - 1;
-                const u32 b0 = __shfl_sync(0xffffffffu, beg, j), d0 = __shfl_sync(0xffffffffu, deg, j);
-                for (u32 i0 = 0; i0 < d0; i0 += 32 * 4) {
-                    u32 wv[4];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const u32 i = i0 + c * 32 + lane;
-                        wv[c] = i < d0 ? __ldg(val + b0 + i) : ~0u;
-                    }
-#pragma unroll
-                    for (int c = 0; c < 4; ++c)
-                        if (wv[c] != ~0u) atomicOr(&row[wv[c] >> 5], 1u << (wv[c] & 31));
-                }
-            }
-            // the other non-empty rows, compacted to the low lanes: windows of
-            // 32 join words; the rows starting in a window are a bit mask, and
-            // a word's row is the number of rows started up to its position
-            if (deg >= 32) deg = 0;
+            // the non-empty rows, compacted to the low lanes: windows of 32 join
+            // words; the rows starting in a window are a bit mask, and a word's
+            // row is the number of rows started up to its position
             const u32 nz = __ballot_sync(0xffffffffu, deg != 0);
             if (nz) {
                 if (deg) {
