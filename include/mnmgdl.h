@@ -137,7 +137,8 @@ typedef struct dl_tuning {
     double hash_load_factor;      /* dl_build_hash_table's default load factor (0 < lf < 1, default 0.5) */
     int32_t join_first_pass;      /* TC: 1 = the join emit also does the sort's first radix pass (default), 0 = not */
     int32_t bitmap_max_gib;       /* TC dedup AUTO: largest bit matrix + transpose, GiB (0..1024, default 48; 0 = never) */
-    int32_t reserved[2];
+    int32_t bitmap_unit_rows;     /* bit-matrix TC: delta rows per work unit (1..16777216, default 65536) */
+    int32_t reserved[1];
 } dl_tuning;
 DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out);
 DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *tuning);

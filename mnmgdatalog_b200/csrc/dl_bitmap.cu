@@ -13,8 +13,10 @@
 // transpose, row popcounts, a scan and an extraction pass.
 //
 // A delta is kept as units: one source x and a run of path targets y (u32,
-// at most UNIT_ROWS of them). Almost all join output of a TC iteration
-// belongs to a few heavy (x, iteration) pairs, so a CTA takes a unit, ORs
+// at most `unit_rows` of them; Tuning::bitmap_unit_rows, default 65,536: a
+// unit costs one fold of the whole row, so fewer, larger units are cheaper).
+// Almost all join output of a TC iteration belongs to a few heavy
+// (x, iteration) pairs, so a CTA takes a unit, ORs
 // the join words (x, w) for every edge y -> w into a shared-memory copy of
 // row x, and then folds that row into M with one atomicOr per touched word
 // (consecutive words: coalesced), instead of one global atomic per join word.
@@ -29,7 +31,6 @@ namespace {
 constexpr int TR_ROWS = 512;  // source rows per transpose tile
 constexpr int TR_WORDS = 16;  // source words (512 columns) per transpose tile
 constexpr int UT = 512;       // threads of the unit kernel
-constexpr u64 UNIT_ROWS = 65536;  // fewer, larger units: each costs a fold of the whole row
 
 // One source x and delta rows rows[start, start + len): paths x -> rows[i].
 struct Unit {
@@ -50,17 +51,17 @@ __global__ void bitmat_set_edges_kernel(const u64 *__restrict__ words, u64 n, in
 }
 
 // Units of the first delta (the edges, from the CSR): per[x] = units of x.
-__global__ void units_per_source_kernel(const u32 *__restrict__ off, u64 n, u64 *__restrict__ per) {
+__global__ void units_per_source_kernel(const u32 *__restrict__ off, u64 n, u64 unit_rows, u64 *__restrict__ per) {
     for (u64 x = (u64) blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (u64) gridDim.x * blockDim.x)
-        per[x] = ((u64) (off[x + 1] - off[x]) + UNIT_ROWS - 1) / UNIT_ROWS;
+        per[x] = ((u64) (off[x + 1] - off[x]) + unit_rows - 1) / unit_rows;
 }
 
-__global__ void units_fill_kernel(const u32 *__restrict__ off, u64 n, const u64 *__restrict__ first,
+__global__ void units_fill_kernel(const u32 *__restrict__ off, u64 n, u64 unit_rows, const u64 *__restrict__ first,
                                   Unit *__restrict__ units) {
     for (u64 x = (u64) blockIdx.x * blockDim.x + threadIdx.x; x < n; x += (u64) gridDim.x * blockDim.x) {
         const u64 b = off[x], e = off[x + 1];
         u64 k = first[x];
-        for (u64 s = b; s < e; s += UNIT_ROWS) units[k++] = Unit{(u32) x, (u32) min(UNIT_ROWS, e - s), s};
+        for (u64 s = b; s < e; s += unit_rows) units[k++] = Unit{(u32) x, (u32) min(unit_rows, e - s), s};
     }
 }
 
@@ -99,7 +100,7 @@ struct StepCounters {
 __global__ void __launch_bounds__(UT, 4)
 bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const u32 *__restrict__ rows,
                         const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
-                        u32 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap,
+                        u32 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap, u64 unit_rows,
                         StepCounters *__restrict__ ctr, u32 *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     UnitSmem &s = *reinterpret_cast<UnitSmem *>(smem_raw);
@@ -219,7 +220,7 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
         u64 dtot;
         block_exclusive_sum<UT / 32>(dsum, s.scratch64, &dtot);
         if (total) {
-            const u64 nsub = (total + UNIT_ROWS - 1) / UNIT_ROWS;
+            const u64 nsub = (total + unit_rows - 1) / unit_rows;
             if (tid == 0) {
                 if (dtot) atomicAdd(&ctr->join, (unsigned long long) dtot);
                 s.obase = atomicAdd(&ctr->units, (unsigned long long) nsub);
@@ -228,7 +229,7 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
             const u64 ub = s.obase;
             for (u64 i = tid; i < nsub; i += UT) {
                 if (ub + i < uout_cap)
-                    uout[ub + i] = Unit{U.x, (u32) min(UNIT_ROWS, total - i * UNIT_ROWS), obase + i * UNIT_ROWS};
+                    uout[ub + i] = Unit{U.x, (u32) min(unit_rows, total - i * unit_rows), obase + i * unit_rows};
                 else
                     atomicOr(err, DL_DEVERR_CAPACITY);
             }
@@ -399,6 +400,7 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
     Workspace &ws = ctx.ws;
     const u64 n = g.n_ids;
     const u64 stride = bitmat_stride(n);
+    const u64 unit_rows = std::max<u64>(1, ctx.tune.bitmap_unit_rows);
     const u64 words_used = (n + 31) / 32;
     const size_t smem = sizeof(UnitSmem) + words_used * 4 + 16;
     if (smem > 227 * 1024) throw Error(DL_ERR_OUT_OF_MEMORY, "bit-matrix rows of " + std::to_string(n) +
@@ -419,12 +421,12 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         ctx.reserve(ws.w0, (n + 1) * 8);
         ctx.reserve(ws.w1, (n + 1) * 8);
         DL_LAUNCH(ctx, K_PREP, 12.0 * n,
-                  units_per_source_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n,
+                  units_per_source_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, unit_rows,
                                                                                            ws.w0.as<u64>()));
         nunits = exclusive_scan(ctx, ws.w0.as<u64>(), n, ws.w1.as<u64>());
         ctx.reserve(*ubuf, std::max<u64>(nunits, 1) * sizeof(Unit));
         DL_LAUNCH(ctx, K_PREP, 16.0 * nunits,
-                  units_fill_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, ws.w1.as<u64>(),
+                  units_fill_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, unit_rows, ws.w1.as<u64>(),
                                                                                      ubuf->as<Unit>()));
         DL_CUDA(cudaMemsetAsync(&ctr->join, 0, sizeof(u64), ctx.stream));
         DL_LAUNCH(ctx, K_PREP, 8.0 * ne,
@@ -451,7 +453,7 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
             pt.mark(PH_DEDUP);
             DevBuf &obuf = ws.jbuf[slot];
             ctx.reserve(obuf, join * 4);
-            const u64 ucap = nunits + join / UNIT_ROWS + 1;
+            const u64 ucap = nunits + join / unit_rows + 1;
             ctx.reserve(*ubuf_next, ucap * sizeof(Unit));
             DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(StepCounters), ctx.stream));
             const unsigned grid = (unsigned) std::min<u64>(nunits, resident);
@@ -459,7 +461,7 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
             DL_LAUNCH(ctx, K_BITMAP_EXPAND, 4.0 * nrows + 16.0 * nunits + 4.0 * join,
                       kern<<<grid, UT, smem, ctx.stream>>>(g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m,
                                                            stride, (u32) words_used, obuf.as<u32>(), join,
-                                                           ubuf_next->as<Unit>(), ucap, ctr, &ctx.ctrl->err));
+                                                           ubuf_next->as<Unit>(), ucap, unit_rows, ctr, &ctx.ctrl->err));
             DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, ctr, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx.stream));
             ctx.sync();
             nnew = ctx.host_scalars[1];

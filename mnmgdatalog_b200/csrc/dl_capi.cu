@@ -614,6 +614,7 @@ DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out) {
     out->join_first_pass = t.join_first_pass;
     out->hash_load_factor = t.hash_load;
     out->bitmap_max_gib = t.bitmap_max_gib;
+    out->bitmap_unit_rows = (int32_t) t.bitmap_unit_rows;
     return DL_OK;
 }
 
@@ -628,6 +629,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     DL_REQUIRE(t->join_first_pass == 0 || t->join_first_pass == 1, "join_first_pass must be 0 or 1");
     DL_REQUIRE(t->hash_load_factor > 0.0 && t->hash_load_factor < 1.0, "hash_load_factor must be in (0, 1)");
     DL_REQUIRE(t->bitmap_max_gib >= 0 && t->bitmap_max_gib <= 1024, "bitmap_max_gib must be in 0..1024");
+    DL_REQUIRE(t->bitmap_unit_rows >= 1 && t->bitmap_unit_rows <= (1 << 24), "bitmap_unit_rows must be in 1..16777216");
     dl::Tuning &o = ctx->c.tune;
     o.sort_algo = t->sort_algorithm;
     o.rank = t->sort_ranking;
@@ -638,6 +640,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     o.join_first_pass = t->join_first_pass;
     o.hash_load = t->hash_load_factor;
     o.bitmap_max_gib = t->bitmap_max_gib;
+    o.bitmap_unit_rows = (uint32_t) t->bitmap_unit_rows;
     return DL_OK;
 }
 

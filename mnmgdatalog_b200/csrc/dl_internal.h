@@ -124,6 +124,7 @@ struct Tuning {
     u64 small_ratio = 4;        // small run folded when |small| * small_ratio >= |large run|
     double hash_load = 0.5;     // default load factor of dl_build_hash_table
     int bitmap_max_gib = 48;    // TC dedup AUTO: bit matrix and transpose at most this many GiB (0 = never)
+    u32 bitmap_unit_rows = 65536;  // bit-matrix TC: delta rows per unit (one shared-memory row fold each)
 };
 Tuning default_tuning();
 

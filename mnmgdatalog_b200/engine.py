@@ -135,7 +135,8 @@ class Engine:
         check(lib().dl_context_synchronize(self.ctx))
 
     TUNING_FIELDS = ("sort_algorithm", "sort_ranking", "sort_keys_per_thread", "sort_input_tma", "dense_ratio",
-                     "small_ratio", "hash_load_factor", "join_first_pass", "bitmap_max_gib")
+                     "small_ratio", "hash_load_factor", "join_first_pass", "bitmap_max_gib",
+                     "bitmap_unit_rows")
 
     def tuning(self) -> dict:
         """The context's engine knobs (dl_tuning)."""

@@ -151,6 +151,27 @@ def test_tc_dedup_modes_agree_at_scale(engine):
         assert torch.equal(a.rows, b.rows), mode
 
 
+@pytest.mark.parametrize("unit_rows", [1, 7, 64])
+def test_tc_bitmap_small_units(engine, unit_rows):
+    """Work units of a few delta rows: every source's delta is split over many
+    units (and CTAs) and emitted again in split units; the results must not
+    change."""
+    from mnmgdatalog_b200 import graphs
+    before = engine.tuning()
+    inputs = [graphs.chung_lu(n=3000, m=10000, seed=2), graphs.dag(n=2000, extra=700, seed=4)]
+    inputs += [load_input(f) for f in TC_FILES if len(load_input(f)) <= 20000][:3]
+    try:
+        engine.set_tuning(bitmap_unit_rows=unit_rows)
+        for k, e in enumerate(inputs):
+            a = engine.tc(e, dedup="sort")
+            b = engine.tc(e, dedup="bitmap")
+            assert a.deltas.tolist() == b.deltas.tolist(), k
+            assert a.join_rows_total == b.join_rows_total, k
+            assert np.array_equal(a.rows, b.rows), k
+    finally:
+        engine.set_tuning(before)
+
+
 def test_tc_bitmap_max_iterations_and_selection(engine):
     """The bit-matrix path stops where the sort path stops, and AUTO picks it
     only while tuning allows (bitmap_max_gib = 0 turns it off)."""

@@ -19,7 +19,7 @@ def test_tuning_round_trip_and_validation(engine):
         assert (t["dense_ratio"], t["small_ratio"], t["hash_load_factor"]) == (8, 2, 0.7)
         for bad in ({"dense_ratio": 0}, {"small_ratio": 65}, {"sort_algorithm": 2}, {"sort_keys_per_thread": 8},
                     {"hash_load_factor": 1.0}, {"sort_input_tma": 2}, {"join_first_pass": 3},
-                    {"bitmap_max_gib": -1}, {"bitmap_max_gib": 1025}):
+                    {"bitmap_max_gib": -1}, {"bitmap_max_gib": 1025}, {"bitmap_unit_rows": 0}):
             with pytest.raises(DatalogError):
                 engine.set_tuning(**bad)
         with pytest.raises(DatalogError):
