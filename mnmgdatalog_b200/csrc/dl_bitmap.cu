@@ -320,10 +320,14 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_kernel(const u32 *_
         const u32 *row = t + w * stride;
         u64 pos = first[w];
         const u64 hi = w << bits;
+        // stride is a multiple of 32 words: a lane's vector stays in the row
+        uint4 nxt = make_uint4(0, 0, 0, 0);
+        if ((u64) lane * 4 < words) nxt = __ldcs(reinterpret_cast<const uint4 *>(row + lane * 4));
         for (u64 k0 = 0; k0 < words; k0 += 128) {
-            const u64 k = k0 + lane * 4;  // stride is a multiple of 32 words: the vector stays in the row
-            uint4 q = make_uint4(0, 0, 0, 0);
-            if (k < words) q = __ldcs(reinterpret_cast<const uint4 *>(row + k));
+            const u64 k = k0 + lane * 4;
+            const uint4 q = nxt;  // this step's words; the next step's load is in flight meanwhile
+            nxt = make_uint4(0, 0, 0, 0);
+            if (k + 128 < words) nxt = __ldcs(reinterpret_cast<const uint4 *>(row + k + 128));
             u32 v[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
             for (int c = 0; c < 4; ++c)
