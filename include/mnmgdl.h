@@ -123,6 +123,11 @@ DL_API const char *dl_version(void);
 DL_API dl_status dl_context_create(int32_t device, void *stream, dl_context **out);
 DL_API dl_status dl_context_destroy(dl_context *ctx);
 DL_API dl_status dl_context_synchronize(dl_context *ctx);
+/* Waits for the context's stream, then frees the device memory the context keeps between
+ * calls: its workspace and cached buffers (e.g. the bit matrix of the last TC run, 2 x n*n/8
+ * bytes). Results of live runs and sessions are not touched; the next call allocates again.
+ * No counterpart in the reference (its drivers free everything per iteration). */
+DL_API dl_status dl_context_release_memory(dl_context *ctx);
 DL_API dl_status dl_free(dl_context *ctx, void *device_ptr);
 
 /* Engine knobs of a context (no counterpart in the reference; set by the

@@ -25,7 +25,7 @@ DEDUP_AUTO, DEDUP_SORT, DEDUP_HASH, DEDUP_BITMAP = 0, 1, 2, 3
 # Every symbol include/mnmgdl.h declares (checked by the CPU test suite).
 EXPORTS = (
     "dl_status_string", "dl_last_error", "dl_version",
-    "dl_context_create", "dl_context_destroy", "dl_context_synchronize", "dl_free", "dl_memcpy",
+    "dl_context_create", "dl_context_destroy", "dl_context_synchronize", "dl_context_release_memory", "dl_free", "dl_memcpy",
     "dl_context_get_tuning", "dl_context_set_tuning",
     "dl_sort_unique", "dl_sort", "dl_set_difference", "dl_merge", "dl_diff_merge",
     "dl_unique_by_key_min", "dl_remove_self_pairs",
@@ -93,6 +93,7 @@ def lib():
         "dl_context_create": ([i32, vp, pvp], C.c_int),
         "dl_context_destroy": ([vp], C.c_int),
         "dl_context_synchronize": ([vp], C.c_int),
+        "dl_context_release_memory": ([vp], C.c_int),
         "dl_free": ([vp, vp], C.c_int),
         "dl_memcpy": ([vp, vp, vp, i64], C.c_int),
         "dl_context_get_tuning": ([vp, C.POINTER(dl_tuning)], C.c_int),

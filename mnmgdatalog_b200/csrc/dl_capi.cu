@@ -170,6 +170,15 @@ DL_API dl_status dl_context_synchronize(dl_context *ctx) {
     });
 }
 
+DL_API dl_status dl_context_release_memory(dl_context *ctx) {
+    DL_REQUIRE(ctx, "ctx is NULL");
+    return guarded([&] {
+        set_device(ctx);
+        ctx->c.sync();
+        ctx->c.release_all();
+    });
+}
+
 DL_API dl_status dl_free(dl_context *ctx, void *p) {
     DL_REQUIRE(ctx, "ctx is NULL");
     if (!p) return DL_OK;

@@ -134,6 +134,11 @@ class Engine:
     def synchronize(self):
         check(lib().dl_context_synchronize(self.ctx))
 
+    def release_memory(self):
+        """Free the device memory the context keeps between calls (workspace,
+        cached buffers, the last TC run's bit matrix); live results stay."""
+        check(lib().dl_context_release_memory(self.ctx))
+
     TUNING_FIELDS = ("sort_algorithm", "sort_ranking", "sort_keys_per_thread", "sort_input_tma", "dense_ratio",
                      "small_ratio", "hash_load_factor", "join_first_pass", "bitmap_max_gib",
                      "bitmap_unit_rows")

@@ -106,6 +106,28 @@ def test_repeated_runs_reuse_buffers(engine):
         assert np.array_equal(r.rows, first.rows)
 
 
+def test_release_memory_between_runs(engine):
+    """The context gives its cached device memory back and the next runs
+    allocate again, with the same results; a result held across the release
+    stays valid."""
+    import torch
+    from mnmgdatalog_b200 import graphs
+    e = graphs.chung_lu(n=4000, m=13000, seed=6)
+    first = engine.tc(e, output="device")
+    before = first.rows.clone()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    engine.release_memory()
+    assert torch.cuda.mem_get_info()[0] >= free0
+    assert torch.equal(first.rows, before)
+    again = engine.tc(e)
+    assert np.array_equal(again.rows, before.cpu().numpy())
+    assert again.deltas.tolist() == first.deltas.tolist()
+    sg = engine.sg(e[:3000])
+    engine.release_memory()
+    assert np.array_equal(engine.sg(e[:3000]).rows, sg.rows)
+
+
 def test_phase_timing(engine):
     r = engine.tc(load_input("data_7035.bin"), phase_timing=True)
     assert r.seconds > 0 and set(r.phases) == {"initialization", "join", "deduplication", "merge",
