@@ -20,7 +20,9 @@
 // the join words (x, w) for every edge y -> w into a shared-memory copy of
 // row x, and then folds that row into M with one atomicOr per touched word
 // (consecutive words: coalesced), instead of one global atomic per join word.
-// The new bits of the unit are its part of the next delta.
+// The new bits of the unit are its part of the next delta: all of them count
+// in |delta|, and those whose target has out-edges (the only ones that can
+// join next step) become its rows.
 #include "dl_engine_detail.h"
 #include "dl_join.cuh"
 
@@ -94,14 +96,27 @@ struct StepCounters {
     unsigned long long words;   // new tuples (next delta rows)
     unsigned long long join;    // join size of the next step
     unsigned long long units;   // units of the next delta
+    unsigned long long fresh;   // new tuples (|delta|; rows are written only for targets with out-edges)
 };
+
+// hasout[k] bit b = node 32 k + b has out-edges (only those can join next step).
+__global__ void hasout_kernel(const u32 *__restrict__ off, u64 n, u64 words, u32 *__restrict__ hasout) {
+    for (u64 k = (u64) blockIdx.x * blockDim.x + threadIdx.x; k < words; k += (u64) gridDim.x * blockDim.x) {
+        u32 v = 0;
+        for (u32 b = 0; b < 32; ++b) {
+            const u64 x = k * 32 + b;
+            if (x < n && off[x + 1] > off[x]) v |= 1u << b;
+        }
+        hasout[k] = v;
+    }
+}
 
 // One semi-naive TC step over the units of a delta (persistent CTAs).
 __global__ void __launch_bounds__(UT, 4)
 bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const u32 *__restrict__ rows,
                         const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
                         u32 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap, u64 unit_rows,
-                        StepCounters *__restrict__ ctr, u32 *err) {
+                        const u32 *__restrict__ hasout, StepCounters *__restrict__ ctr, u32 *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     UnitSmem &s = *reinterpret_cast<UnitSmem *>(smem_raw);
     u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(UnitSmem));
@@ -167,9 +182,11 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
         }
         __syncthreads();
         // ---- fold the row into M: new bits = row & ~M ----
+        // Every new bit counts in |delta|; only targets with out-edges become
+        // rows of the next delta (the others can join nothing).
         const u32 lim = words;  // the whole row, in order: coalesced atomics on M
         const u64 mrow = (u64) U.x * stride;
-        u32 cnt = 0;
+        u64 cnt = 0;  // (new bits << 32) | new rows
         for (u32 q0 = 0; q0 < lim; q0 += UT * 4) {
             u32 kk[4], v[4], old[4];
 #pragma unroll
@@ -184,14 +201,19 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
             for (int c = 0; c < 4; ++c) {
                 if (v[c]) {
                     const u32 f = v[c] & ~old[c];
-                    row[kk[c]] = f;
-                    cnt += __popc(f);
+                    const u32 fr = f ? f & __ldg(hasout + kk[c]) : 0u;
+                    row[kk[c]] = fr;
+                    cnt += ((u64) __popc(f) << 32) | __popc(fr);
                 }
             }
         }
-        u32 total;
-        u32 pos = block_exclusive_sum<UT / 32>(cnt, s.scratch, &total);
-        if (tid == 0) s.obase = total ? atomicAdd(&ctr->words, (unsigned long long) total) : 0ull;
+        u64 both;
+        const u32 pos = (u32) block_exclusive_sum<UT / 32>(cnt, s.scratch64, &both);
+        const u32 total = (u32) both;  // new rows of the unit
+        if (tid == 0) {
+            s.obase = total ? atomicAdd(&ctr->words, (unsigned long long) total) : 0ull;
+            if (both >> 32) atomicAdd(&ctr->fresh, both >> 32);
+        }
         __syncthreads();
         // ---- emit the new tuples (targets of x), clear the row ----
         const u64 obase = s.obase;
@@ -440,6 +462,10 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         ctx.sync();
         join = ctx.host_scalars[0];
     }
+    ctx.reserve(ws.bit_hasout, std::max<u64>(words_used, 1) * 4);
+    DL_LAUNCH(ctx, K_PREP, 4.0 * n + 4.0 * words_used,
+              hasout_kernel<<<grid_for(words_used, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, words_used,
+                                                                                      ws.bit_hasout.as<u32>()));
     u64 nfull = ne;
     u64 nrows = ne;  // rows of the current delta
     auto kern = bitmat_unit_step_kernel;
@@ -465,15 +491,17 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
             DL_LAUNCH(ctx, K_BITMAP_EXPAND, 4.0 * nrows + 16.0 * nunits + 4.0 * join,
                       kern<<<grid, UT, smem, ctx.stream>>>(g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m,
                                                            stride, (u32) words_used, obuf.as<u32>(), join,
-                                                           ubuf_next->as<Unit>(), ucap, unit_rows, ctr, &ctx.ctrl->err));
+                                                           ubuf_next->as<Unit>(), ucap, unit_rows,
+                                                           ws.bit_hasout.as<u32>(), ctr, &ctx.ctrl->err));
             DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, ctr, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx.stream));
             ctx.sync();
-            nnew = ctx.host_scalars[1];
+            const u64 next_rows = ctx.host_scalars[1];
             next_join = ctx.host_scalars[2];
             next_units = ctx.host_scalars[3];
-            ctx.prof_add_bytes(K_BITMAP_EXPAND, 4.0 * nnew + 16.0 * next_units);
+            nnew = ctx.host_scalars[4];
+            ctx.prof_add_bytes(K_BITMAP_EXPAND, 4.0 * next_rows + 16.0 * next_units);
             rows = obuf.as<u32>();
-            nrows = nnew;
+            nrows = next_rows;
             slot ^= 1;
             std::swap(ubuf, ubuf_next);
         }

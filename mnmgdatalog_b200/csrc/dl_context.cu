@@ -116,7 +116,7 @@ void Context::release_all() {
     DevBuf *all[] = {&ws.input, &ws.ids, &ws.w0, &ws.w1, &ws.csr_off, &ws.csr_val, &ws.full[0], &ws.full[1],
                      &ws.small[0], &ws.small[1], &ws.tiny[0], &ws.tiny[1], &ws.sample, &ws.sample_small,
                      &ws.jbuf[0], &ws.jbuf[1], &ws.offsets, &ws.wcc_label, &ws.wcc_flag, &ws.wcc_next,
-                     &ws.bitmat[0], &ws.bitmat[1], &ws.offsets_next,
+                     &ws.bitmat[0], &ws.bitmat[1], &ws.offsets_next, &ws.bit_hasout,
                      &lookback, &sort_hist, &lbs_splits, &radix_part, &merge_splits, &bucket_cursor};
     for (DevBuf *b : all) b->release();
 }

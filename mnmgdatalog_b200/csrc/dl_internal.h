@@ -109,6 +109,7 @@ struct Workspace {
     DevBuf offsets_next;   // bit-matrix TC: the next delta's join offsets
     DevBuf wcc_label, wcc_flag, wcc_next;
     DevBuf bitmat[2];      // TC full relation as a bit matrix; its transpose
+    DevBuf bit_hasout;     // bit-matrix TC: nodes with out-edges (one bit each)
 };
 
 // Engine knobs the autotuner sets per context (mnmgdatalog_b200/autotune.py);
