@@ -263,14 +263,19 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
 
 // Lane l gets the word whose bit b is bit l of lane b's word (32 x 32 bit
 // transpose by recursive block swaps: each stage exchanges bit j of the row
-// index with bit j of the column index).
+// index with bit j of the column index). The 16- and 8-bit stages move whole
+// bytes, so one byte permute does each.
 __device__ __forceinline__ u32 transpose32(u32 v, u32 lane) {
-    const u32 masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+    u32 u = __shfl_xor_sync(0xffffffffu, v, 16);
+    v = __byte_perm(v, u, (lane & 16) ? 0x3276 : 0x5410);
+    u = __shfl_xor_sync(0xffffffffu, v, 8);
+    v = __byte_perm(v, u, (lane & 8) ? 0x3715 : 0x6240);
+    const u32 masks[3] = {0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
 #pragma unroll
-    for (int s = 0; s < 5; ++s) {
-        const int j = 16 >> s;
+    for (int s = 0; s < 3; ++s) {
+        const int j = 4 >> s;
         const u32 mk = masks[s];
-        const u32 u = __shfl_xor_sync(0xffffffffu, v, j);
+        u = __shfl_xor_sync(0xffffffffu, v, j);
         v = (lane & j) ? ((v & ~mk) | ((u >> j) & mk)) : ((v & mk) | ((u & mk) << j));
     }
     return v;
