@@ -34,6 +34,7 @@ typedef int64_t MPI_Offset;
 #define MPI_INFO_NULL 0
 #define MPI_STATUS_IGNORE ((MPI_Status *) 0)
 #define MPI_MAX_ERROR_STRING 256
+#define MPI_ERR_COUNT 2
 
 #define MPI_INT 1
 #define MPI_LONG 2
@@ -128,6 +129,7 @@ static inline int MPI_File_close(MPI_File *fh) {
     return MPI_SUCCESS;
 }
 static inline int MPI_File_read_at(MPI_File fh, MPI_Offset off, void *buf, int count, MPI_Datatype t, MPI_Status *) {
+    if (count < 0) return MPI_ERR_COUNT; /* as MPI does; nothing is read */
     size_t want = (size_t) count * mpi_stub_type_size(t), got = 0;
     while (got < want) {
         ssize_t k = pread(fh->fd, (char *) buf + got, want - got, (off_t) off + (off_t) got);
@@ -137,6 +139,9 @@ static inline int MPI_File_read_at(MPI_File fh, MPI_Offset off, void *buf, int c
     return MPI_SUCCESS;
 }
 static inline int MPI_File_write_at(MPI_File fh, MPI_Offset off, const void *buf, int count, MPI_Datatype t, MPI_Status *) {
+    /* A count that overflowed int (the reference passes rows * 2 as an int)
+     * is rejected as MPI rejects it: nothing is written. */
+    if (count < 0) return MPI_ERR_COUNT;
     size_t want = (size_t) count * mpi_stub_type_size(t), put = 0;
     while (put < want) {
         ssize_t k = pwrite(fh->fd, (const char *) buf + put, want - put, (off_t) off + (off_t) put);
