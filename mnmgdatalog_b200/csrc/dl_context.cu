@@ -13,6 +13,9 @@ double now_s() {
 
 void DevBuf::reserve(size_t bytes, bool zero) {
     if (bytes <= cap && p) return;
+    if (fixed)
+        throw Error(DL_ERR_INTERNAL, "a fixed scratch slice of " + std::to_string(cap) + " bytes cannot hold " +
+                                         std::to_string(bytes) + " bytes");
     size_t want = bytes + bytes / 8 + 256;
     release();
     cudaError_t e = cudaMalloc(&p, want);
@@ -28,12 +31,18 @@ void DevBuf::reserve(size_t bytes, bool zero) {
 }
 
 void DevBuf::release() {
+    if (fixed) return;  // not ours to free
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
 }
 
 void Context::reserve(DevBuf &buf, size_t bytes, bool zero) {
+    if (buf.fixed) {  // a fixed slice: it fits or the request is an error
+        buf.reserve(bytes);
+        if (zero) DL_CUDA(cudaMemsetAsync(buf.p, 0, buf.cap, stream));
+        return;
+    }
     if (buf.p && buf.cap >= bytes) return;
     // A buffer that outgrows itself grows by half at least, so a relation that
     // grows every iteration is reallocated O(log) times, not at every step.
@@ -64,6 +73,9 @@ void Context::reserve(DevBuf &buf, size_t bytes, bool zero) {
 }
 
 void Context::allocate(DevBuf &buf, size_t bytes, bool zero, size_t minimum) {
+    if (no_alloc)
+        throw Error(DL_ERR_INTERNAL, "a context without allocation was asked for a new buffer of " +
+                                         std::to_string(bytes) + " bytes");
     const double t0 = now_s();
     try {
         buf.reserve(bytes, zero);
@@ -101,7 +113,7 @@ void Context::trim_spares() {
 }
 
 void Context::give_back(DevBuf &buf) {
-    if (!buf.p) return;
+    if (!buf.p || buf.fixed) return;
     spares.push_back(buf);
     buf = DevBuf();
     trim_spares();
@@ -117,7 +129,8 @@ void Context::release_all() {
                      &ws.small[0], &ws.small[1], &ws.tiny[0], &ws.tiny[1], &ws.sample, &ws.sample_small,
                      &ws.jbuf[0], &ws.jbuf[1], &ws.offsets, &ws.wcc_label, &ws.wcc_flag, &ws.wcc_next,
                      &ws.bitmat[0], &ws.bitmat[1], &ws.offsets_next, &ws.bit_hasout,
-                     &lookback, &sort_hist, &lbs_splits, &radix_part, &merge_splits, &bucket_cursor};
+                     &lookback, &sort_hist, &lbs_splits, &radix_part, &merge_splits, &bucket_cursor,
+                     &part_cursor};
     for (DevBuf *b : all) b->release();
 }
 
@@ -157,7 +170,7 @@ const char *kernel_name(int kid) {
     static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_spine_scan", "sort_scatter_pass",
                                          "select_compact", "join_count_scan", "join_partition", "join_emit",
                                          "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build",
-                                         "sparse_diff", "hash_insert", "bitmap_expand", "bitmap_extract", "host_cudaMalloc", "host_cudaFree",
+                                         "sparse_diff", "hash_insert", "bitmap_expand", "bitmap_transpose", "bitmap_extract", "host_cudaMalloc", "host_cudaFree",
                                          "host_sync"};
     return (kid >= 0 && kid < K_COUNT) ? names[kid] : "?";
 }
