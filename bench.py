@@ -41,6 +41,7 @@ L2_FLUSH_BYTES = 256 << 20
 CPU_SAMPLE_NODES = 8000      # cpu_baseline sample (~15-25 s on one core)
 REF_SAMPLE_NODES = 6000      # reference arm sample per step (~5-10 s)
 HBM_FALLBACK_GBS = 6650.0
+TUNING_BATCH = os.path.join(ROOT, "mnmgdatalog_b200", "tuning_batch.json")
 
 
 def _env_int(k, d):
@@ -158,6 +159,31 @@ def run_tc_mpi_sample(nodes: int, seed: int = 0) -> dict:
             "tuples": tuples, "seconds": secs}
 
 
+def run_reference_gpu(prog: str, edges: np.ndarray, timeout: int = 600) -> dict:
+    """Context figure: the reference's own GPU program (tc.cu / sg.cu built
+    unmodified by oracle/Makefile into oracle/_ref/, one MPI rank) on the same
+    input on this GPU, job_run=1 (no output file). Its "Total Time" column
+    excludes file I/O (tc.cu:387-389); the engine's `value` covers the same
+    span (input upload through the unpacked result rows)."""
+    binary = os.path.join(ROOT, "oracle", "_ref", f"{prog}.out")
+    if not os.path.exists(binary):
+        return {"unavailable": f"oracle/_ref/{prog}.out not built"}
+    with tempfile.TemporaryDirectory() as td:
+        inp = os.path.join(td, "input.bin")
+        edges.astype("<i4").tofile(inp)
+        t0 = time.perf_counter()
+        r = subprocess.run([binary, inp, "0", "0", "1"], capture_output=True, text=True, timeout=timeout, cwd=td)
+        wall = time.perf_counter() - t0
+    if r.returncode != 0:
+        return {"error": f"exit {r.returncode}: {r.stderr[-300:]}"}
+    csv = [l for l in r.stdout.splitlines() if l and l[0].isdigit()][-1].split(",")
+    total = float(csv[4])
+    return {"program": f"oracle/_ref/{prog}.out <input> 0 0 1 (reference {prog}.cu, unmodified, one MPI rank)",
+            "iterations": int(csv[2]), "tuples": int(csv[3]), "total_s": total,
+            "tuples_per_s": int(csv[3]) / total if total > 0 else None, "wall_s": round(wall, 2),
+            "note": "context only; the reference arm of this benchmark is the CPU program"}
+
+
 def main_reference(args, rank: int, world: int) -> int:
     if rank != 0:
         return 0
@@ -182,38 +208,33 @@ def main_reference(args, rank: int, world: int) -> int:
     return 0
 
 
-def main_ours(args, rank: int, world: int, local_rank: int) -> int:
+def timed_fixpoints(eng, prog, d_edges, steps, warmup, dedup, dev, world, barrier, flush, clocks=None):
+    """`warmup` untimed and `steps` timed whole fixpoints of one program on
+    edges already in HBM; each step ends with the result rows in the
+    reference's file order in device memory (the rank -> id unpack the
+    reference times as finalization, tc.cu:319-327; the destination is
+    allocated once). L2 is flushed between steps, outside the events.
+    Returns (per-step ms on this rank, last result, live profile)."""
     import torch
-    import torch.distributed as dist
-
-    from mnmgdatalog_b200 import Engine
-
-    torch.cuda.set_device(local_rank)
-    dev = torch.device("cuda", local_rank)
-    prog, edges = workload(args.config)
-    stream = torch.cuda.Stream(device=dev)
-    eng = Engine(local_rank, stream=stream)
-    d_edges = torch.from_numpy(edges).to(dev)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    first = eng.run(prog, d_edges, output="none", dedup=dedup)
+    out_rows = torch.empty((max(first.output_tuples, 1), 2), dtype=torch.int32, device=dev)
+    del first
 
     def step():
-        return eng.run(prog, d_edges, output="none", dedup=args.dedup)
+        return eng.run(prog, d_edges, output="device", out=out_rows, dedup=dedup)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
-    clocks = ClockSampler(local_rank)
-    clocks.start()
+    if clocks:
+        clocks.start()
     eng.profile(True)
+    stream = eng._stream_obj
     evs = []
-    tuples = 0
-    for _ in range(args.steps):
+    r = None
+    for _ in range(steps):
         with torch.cuda.stream(stream):
             flush.fill_(1)                      # L2 flush, outside the timed events
             a = torch.cuda.Event(enable_timing=True)
@@ -223,34 +244,84 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
         with torch.cuda.stream(stream):
             b.record(stream)
         evs.append((a, b))
-        tuples += r.output_tuples
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
-    clk = clocks.stop()
     prof = eng.profile_read()
     eng.profile(False)
-    my_ms = sum(a.elapsed_time(b) for a, b in evs)
-    max_ms, total = combine_ranks(my_ms, float(tuples), world, dev)
-    value = total / (max_ms / 1e3)
+    ms = [a.elapsed_time(b) for a, b in evs]
+    r.rows = None
+    del out_rows
+    return ms, r, prof
 
-    # dominant kernel class by device time over the timed region
+
+def roofline_of(prof: dict, step_s: float) -> tuple[dict, dict, dict, int]:
+    """The dominant kernel class by device time: its algorithmic bytes per
+    event-timed second against the measured HBM peak."""
     peak, peak_kind = measured_peak_gbs()
     host = {k: v for k, v in prof.items() if k.startswith("host_")}
     prof = {k: v for k, v in prof.items() if not k.startswith("host_")}
     dom_name, dom = max(((k, v) for k, v in prof.items() if v["timed_launches"]), key=lambda kv: kv[1]["seconds"])
     launches = sum(v["launches"] for v in prof.values())
     achieved = dom["bytes"] / dom["seconds"] / 1e9 if dom["seconds"] else 0.0
-    traffic = traffic_per_launch(dom_name, dom)
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": traffic, "launches": dom["timed_launches"],
-                "share_of_step": dom["seconds"] / (my_ms / 1e3),
+                "traffic": traffic_per_launch(dom_name, dom), "launches": dom["timed_launches"],
+                "share_of_step": dom["seconds"] / step_s if step_s else None,
                 "algorithmic_bytes_per_launch": dom["bytes"] / max(dom["timed_launches"], 1)}
     kernels = {k: {"launches": v["launches"], "ms": round(1e3 * v["seconds"], 3), "bytes": v["bytes"],
-                   "GBps": round(v["bytes"] / v["seconds"] / 1e9, 1) if v["seconds"] else None}
+                   "GBps": round(v["bytes"] / v["seconds"] / 1e9, 1) if v["seconds"] else None,
+                   "frac": round(v["bytes"] / v["seconds"] / 1e9 / peak, 4) if v["seconds"] else None}
                for k, v in prof.items() if v["launches"]}
     host_costs = {k: {"calls": v["launches"], "ms": round(1e3 * v["seconds"], 3)} for k, v in host.items()}
+    return roofline, kernels, host_costs, launches
+
+
+def release(eng, torch):
+    """Hand a context's cached device memory back between legs, so that one
+    leg's buffers neither crowd out nor speed up the next."""
+    eng.release_memory()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+
+def main_ours(args, rank: int, world: int, local_rank: int) -> int:
+    import torch
+    import torch.distributed as dist
+
+    from mnmgdatalog_b200 import Engine
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    prog, edges = workload(args.config)
+
+    # The reference's own GPU program on the same input, first, while the
+    # device is empty (context figure, rank 0 of a one-GPU run only).
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu and prog in ("tc", "sg"):
+        try:
+            ref_gpu = run_reference_gpu(prog, edges)
+        except Exception as exc:  # report, never hide
+            ref_gpu = {"error": f"{type(exc).__name__}: {exc}"}
+
+    stream = torch.cuda.Stream(device=dev)
+    eng = Engine(local_rank, stream=stream)
+    d_edges = torch.from_numpy(edges).to(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    clocks = ClockSampler(local_rank)
+    ms, r, prof = timed_fixpoints(eng, prog, d_edges, args.steps, args.warmup, args.dedup, dev, world, barrier,
+                                  flush, clocks)
+    clk = clocks.stop()
+    my_ms = sum(ms)
+    max_ms, total = combine_ranks(my_ms, float(r.output_tuples * args.steps), world, dev)
+    value = total / (max_ms / 1e3)
+    roofline, kernels, host_costs, launches = roofline_of(prof, my_ms / 1e3)
+    release(eng, torch)
 
     e2e = None
     if not args.no_e2e:
@@ -258,19 +329,33 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
             e2e = measure_e2e(eng, prog, edges, args, dev, world, barrier)
         except Exception as exc:  # reported in the line, never hidden
             e2e = {"value": None, "unit": UNIT, "error": f"{type(exc).__name__}: {exc}"}
+        release(eng, torch)
+    del d_edges
+
+    sg = None
+    if args.sg_leg and world == 1:
+        try:
+            sg = measure_sg_dataset(eng, args, dev, flush)
+        except Exception as exc:  # reported in the line, never hidden
+            sg = {"error": f"{type(exc).__name__}: {exc}"}
+        release(eng, torch)
 
     batched = served = None
     if args.batch_instances > 0:
         try:
-            batched = measure_batched(eng, dev, args)
+            with Engine(local_rank) as beng:
+                batched = measure_batched(beng, dev, args)
         except Exception as exc:  # reported in the line, never hidden
             batched = {"error": f"{type(exc).__name__}: {exc}"}
+        torch.cuda.empty_cache()
     if args.serve_requests > 0:
         try:
             tuned = batched.get("tuning") if isinstance(batched, dict) else None
-            served = measure_served(eng, args, tuned)
+            with Engine(local_rank) as seng:
+                served = measure_served(seng, args, tuned)
         except Exception as exc:
             served = {"error": f"{type(exc).__name__}: {exc}"}
+        torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -279,21 +364,57 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
             cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as exc:  # report, never hide
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {exc}"}
+        cpu["host_cores"] = os.cpu_count()
 
     if rank == 0:
         cfg = describe(args.config, edges)
         cfg.update({"parallelism": f"replicas x{world}", "l2": "256 MiB write between steps (outside timing)",
                     "output_tuples_per_step": int(r.output_tuples), "iterations": int(r.iterations),
-                    "join_rows_per_step": int(r.join_rows_total), "join_rows_max_iteration": int(r.join_rows_max)})
+                    "join_rows_per_step": int(r.join_rows_total), "join_rows_max_iteration": int(r.join_rows_max),
+                    "step": "input edges in HBM -> fixpoint -> result rows (reference file order) in HBM"})
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
                 "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clk, "kernels": kernels, "host": host_costs,
+                "step_ms": [round(x, 3) for x in ms], "reference_gpu": ref_gpu, "sg": sg,
                 "batched": batched, "served": served}
         print(json.dumps(line))
     eng.close()
     return 0
+
+
+SG_DATASET = ("data_163734.bin", "fe_body", 408_443_204, 125, "logs/small-merged-job-output.txt:212")
+
+
+def load_fixture(name: str) -> np.ndarray:
+    import gzip
+    with gzip.open(os.path.join(ROOT, "tests", "golden", "data", name + ".gz"), "rb") as f:
+        raw = f.read()
+    return np.frombuffer(raw, dtype="<i4")[: (len(raw) // 8) * 2].reshape(-1, 2).copy()
+
+
+def measure_sg_dataset(eng, args, dev, flush) -> dict:
+    """SG at 10^8+ tuples: the reference's fe_body input (163,734 edges; the
+    reference published 408,443,204 tuples in 125 iterations), timed like the
+    main leg (device events, result rows in HBM), with the dominant sort-path
+    kernel's roofline and the reference's own GPU program on the same input."""
+    import torch
+    fname, name, pub_tuples, pub_iters, cite = SG_DATASET
+    edges = load_fixture(fname)
+    ref = None
+    if not args.no_reference_gpu:
+        ref = run_reference_gpu("sg", edges)
+    d_edges = torch.from_numpy(edges).to(dev)
+    steps = max(1, min(args.steps, 3))
+    ms, r, prof = timed_fixpoints(eng, "sg", d_edges, steps, 1, "auto", dev, 1, lambda: None, flush)
+    roofline, kernels, _, launches = roofline_of(prof, sum(ms) / 1e3)
+    return {"workload": f"SG on {name} ({fname}, {len(edges)} edges; the reference published {pub_tuples} tuples "
+                        f"in {pub_iters} iterations, {cite})",
+            "value": r.output_tuples * steps / (sum(ms) / 1e3), "unit": UNIT, "steps": steps,
+            "ms_per_step": sum(ms) / steps, "tuples": int(r.output_tuples), "iterations": int(r.iterations),
+            "matches_published": bool(r.output_tuples == pub_tuples and r.iterations == pub_iters),
+            "roofline": roofline, "kernels": kernels, "gpu_launches": launches, "reference_gpu": ref}
 
 
 def traffic_per_launch(kernel: str, stat: dict):
@@ -357,20 +478,32 @@ def measure_batched(eng, dev, args) -> dict:
     work = graphs.batched_workload(count=args.batch_instances, seed=0)
     groups = {p: [torch.from_numpy(e).to(dev) for q, e in work if q == p] for p in ("tc", "wcc")}
     torch.cuda.synchronize(dev)
-    # knobs picked by the autotuner on a sample (every 4th TC instance; its
-    # deltas must not change), then used for the whole batch and the plain runs
+    # The knobs come from the committed record of an autotuner run on this
+    # workload (mnmgdatalog_b200/tuning_batch.json), so that every box runs
+    # the same configuration; --autotune re-runs the autotuner on a sample
+    # (every 4th TC instance; its deltas must not change). Both the batched
+    # and the plain runs use them.
     before = eng.tuning()
-    tuned = autotune.autotune_batch(eng, "tc", groups["tc"][::4], repeats=2, log=lambda *_: None)["tuning"]
+    if args.autotune:
+        tuned = autotune.autotune_batch(eng, "tc", groups["tc"][::4], repeats=2, log=lambda *_: None)["tuning"]
+        source = "autotuned in this run"
+    else:
+        with open(TUNING_BATCH) as f:
+            tuned = json.load(f)["tuning"]
+        source = "mnmgdatalog_b200/tuning_batch.json"
+    eng.set_tuning(tuned)
     for _ in range(max(1, min(args.warmup, 2))):
         for p, g in groups.items():
             eng.run_batch(p, g, output="none")
     eng.synchronize()
-    reps = max(1, min(args.steps, 3))
-    t0 = time.perf_counter()
+    reps = max(5, min(args.steps, 7))
+    times = []
     for _ in range(reps):
+        t0 = time.perf_counter()
         batched = {p: eng.run_batch(p, g, output="none") for p, g in groups.items()}
-    eng.synchronize()
-    t_batch = (time.perf_counter() - t0) / reps
+        eng.synchronize()
+        times.append(time.perf_counter() - t0)
+    t_batch = statistics.median(times)
     t0 = time.perf_counter()
     plain = {p: [eng.run(p, x, output="none") for x in g] for p, g in groups.items()}
     eng.synchronize()
@@ -386,7 +519,9 @@ def measure_batched(eng, dev, args) -> dict:
             "edges_total": int(sum(len(e) for _, e in work)), "tc_tuples": int(tuples),
             "queries_per_s": n / t_batch, "plain_queries_per_s": n / t_plain,
             "speedup_vs_plain": t_plain / t_batch, "seconds": t_batch, "plain_seconds": t_plain,
-            "reps": reps, "identical_to_plain": bool(same), "tuning": tuned,
+            "reps": reps, "batch_seconds": {"median": t_batch, "min": min(times), "max": max(times)},
+            "queries_per_s_range": [n / max(times), n / min(times)],
+            "identical_to_plain": bool(same), "tuning": tuned, "tuning_source": source,
             "timer": "host wall clock around dl_run_batch per program (synchronized), inputs in HBM",
             "form": "union fixpoint per program (one launch sequence per iteration for all instances)"}
 
@@ -398,15 +533,20 @@ def measure_served(eng, args, tuning=None) -> dict:
     one at a time. Capacity is measured with every request queued at t=0;
     the Poisson run uses 80% of it."""
     from mnmgdatalog_b200 import serve
-    reqs = serve.mixed_requests(args.serve_requests, lo=1000, hi=500_000, pool=args.serve_pool, seed=0)
+    reqs = serve.mixed_requests(args.serve_requests, lo=1000, hi=500_000, pool=args.serve_pool, seed=0,
+                                distinct=True)
     for r in reqs[:6]:  # warm-up of every program
         eng.run(r.program, r.edges, output="none")
     before = eng.tuning()
     if tuning:
         eng.set_tuning(tuning)
-    t_plain, svc, _ = serve.serve_plain(eng, reqs, pinned=True, keep_results=False)
+    # the plain engine on an evenly spaced sample of the same stream (one at a
+    # time it would take minutes for all of it); its rate is the comparison
+    every = max(1, len(reqs) // max(1, args.serve_plain_sample))
+    sample = reqs[::every]
+    t_plain, svc, _ = serve.serve_plain(eng, sample, pinned=True, keep_results=False)
     eng.set_tuning(before)
-    plain_qps = len(reqs) / t_plain
+    plain_qps = len(sample) / t_plain
 
     def fresh():
         return [serve.Request(r.id, r.program, r.edges) for r in reqs]
@@ -428,8 +568,11 @@ def measure_served(eng, args, tuning=None) -> dict:
     finally:
         srv.close()
     sp50, sp95, sp99, _ = serve.percentiles(svc)
-    return {"workload": f"{len(reqs)} requests, TC/SG/WCC uniform, edges log-uniform 1K-500K, inputs drawn from "
-                        f"{args.serve_pool} seeded graphs per program, Poisson arrivals at 80% of capacity",
+    return {"workload": f"{len(reqs)} requests, TC/SG/WCC uniform, edges log-uniform 1K-500K "
+                        f"({sum(len(r.edges) for r in reqs)} edges in all); every input distinct: one of "
+                        f"{args.serve_pool} seeded graphs per program under the request's own seeded id map; "
+                        f"Poisson arrivals at 80% of capacity",
+            "plain_sample": f"every {every}th request ({len(sample)})",
             "capacity_queries_per_s": sat.queries_per_s, "plain_queries_per_s": plain_qps,
             "speedup_vs_plain": sat.queries_per_s / plain_qps,
             "poisson_rate": rate, "poisson_queries_per_s": poi.queries_per_s,
@@ -455,11 +598,19 @@ def main(argv=None) -> int:
     ap.add_argument("--config", default="c1_tc_chung_lu")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU program on the same input (context figure)")
     ap.add_argument("--dedup", choices=["auto", "sort", "hash", "bitmap"], default="auto",
                     help="how TC removes known tuples (same results)")
+    ap.add_argument("--no-sg-leg", dest="sg_leg", action="store_false",
+                    help="skip the SG leg on the reference's fe_body input")
     ap.add_argument("--batch-instances", type=int, default=1024, help="batched form instances (0: skip)")
-    ap.add_argument("--serve-requests", type=int, default=600, help="served form requests (0: skip)")
-    ap.add_argument("--serve-pool", type=int, default=32, help="distinct seeded graphs per program")
+    ap.add_argument("--autotune", action="store_true",
+                    help="re-run the autotuner for the batched leg instead of the committed knobs")
+    ap.add_argument("--serve-requests", type=int, default=20000, help="served form requests (0: skip)")
+    ap.add_argument("--serve-pool", type=int, default=64, help="seeded base graphs per program")
+    ap.add_argument("--serve-plain-sample", type=int, default=1000,
+                    help="requests of the stream the plain engine serves one at a time")
     args = ap.parse_args(argv)
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)

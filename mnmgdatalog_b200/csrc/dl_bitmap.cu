@@ -79,15 +79,18 @@ __global__ void edge_degree_sum_kernel(const u32 *__restrict__ off, const u32 *_
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(sum, (unsigned long long) s);
 }
 
+constexpr int UW = UT / 32;   // warps of the unit kernel
+constexpr u32 SCHUNK = 8;     // summary words per warp chunk in the fold and emit phases
+
 struct UnitSmem {
-    u32 wbeg[UT / 32][32];   // per-warp compacted rows: first edge
-    u32 wdeg[UT / 32][32];   // and degree
-    u64 scratch64[UT / 32 + 1];
-    u32 scratch[UT / 32 + 1];
+    u32 wbeg[UW][32];   // per-warp compacted rows: first edge
+    u32 wdeg[UW][32];   // and degree
+    u32 wrows[UW];      // per-warp new rows of the unit (fold phase)
+    u32 wbits[UW];      // per-warp new bits of the unit
     u32 unit;
     u32 next_group;
     unsigned long long obase;
-    // followed by: u32 row[words]
+    // followed by: u32 row[words], u32 summ[swords]
 };
 
 // Counters of one step (device, zeroed before the launch).
@@ -111,7 +114,24 @@ __global__ void hasout_kernel(const u32 *__restrict__ off, u64 n, u64 words, u32
     }
 }
 
+// Next row group of the unit for this warp (lane 0 takes it, all lanes get it).
+__device__ __forceinline__ u32 take_group(UnitSmem &s, u32 lane) {
+    u32 g = 0;
+    if (lane == 0) g = atomicAdd(&s.next_group, 1u);
+    return __shfl_sync(0xffffffffu, g, 0);
+}
+
 // One semi-naive TC step over the units of a delta (persistent CTAs).
+//
+// Per unit (source x, delta rows y): every join word (x, w), w an edge target
+// of a row y, is ORed into a shared-memory copy of row x; a summary bit per
+// 32 row words records which words were touched (set by the lane that first
+// touches a word). The fold then visits only touched words: one atomicOr
+// (with return) on the matrix per word, coalesced over 32 consecutive words;
+// new bits = row & ~old, and those whose target has out-edges become rows of
+// the next delta. The emit visits only words with such rows and writes them
+// warp-cooperatively (one ballot per non-zero word, consecutive positions).
+// Phases are separated by four CTA barriers per unit.
 __global__ void __launch_bounds__(UT, 4)
 bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const u32 *__restrict__ rows,
                         const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
@@ -120,34 +140,38 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
     extern __shared__ __align__(16) unsigned char smem_raw[];
     UnitSmem &s = *reinterpret_cast<UnitSmem *>(smem_raw);
     u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(UnitSmem));
+    const u32 swords = (words + 31) / 32;
+    u32 *summ = row + words;
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const u32 lt = lanemask_lt();
-    for (u32 k = tid; k < words; k += UT) row[k] = 0;
+    const u32 le = lane == 31 ? ~0u : (2u << lane) - 1;  // lanes <= lane
+    const u32 nchunks = (swords + SCHUNK - 1) / SCHUNK;
+    for (u32 k = tid; k < words + swords; k += UT) row[k] = 0;
     if (tid == 0) s.next_group = 0;
     for (;;) {
         if (tid == 0) s.unit = (u32) min((unsigned long long) nunits, atomicAdd(&ctr->fetch, 1ull));
-        __syncthreads();
+        __syncthreads();  // (1) unit taken; row, summary and group counter are clear
         const u64 ui = s.unit;
         if (ui >= nunits) break;
         const Unit U = units[ui];
         // ---- join words (x, w) of the unit into the shared row ----
-        // Warps take groups of 32 rows and expand them 32 join words at a time.
-        for (;;) {
-            u32 grp = 0;
-            if (lane == 0) grp = atomicAdd(&s.next_group, 1u);
-            grp = __shfl_sync(0xffffffffu, grp, 0);
-            const u32 r0 = grp * 32;
-            if (r0 >= U.len) break;
-            const u32 r = r0 + lane;
+        // Warps take groups of 32 rows; the next group's rows are loaded while
+        // the current one is expanded, 32 join words at a time (the rows
+        // starting in a window are a bit mask; a word's row is the number of
+        // rows started up to its position), with the next window's edge-target
+        // load in flight before the current window's shared-memory atomics.
+        u32 grp = take_group(s, lane);
+        u32 ny = 0;
+        if (grp * 32 + lane < U.len) ny = rows[U.start + grp * 32 + lane];
+        while (grp * 32 < U.len) {
+            const u32 r = grp * 32 + lane;
             u32 beg = 0, deg = 0;
             if (r < U.len) {
-                const u32 y = rows[U.start + r];
-                beg = __ldg(off + y);
-                deg = __ldg(off + y + 1) - beg;
+                beg = __ldg(off + ny);
+                deg = __ldg(off + ny + 1) - beg;
             }
-            // the non-empty rows, compacted to the low lanes: windows of 32 join
-            // words; the rows starting in a window are a bit mask, and a word's
-            // row is the number of rows started up to its position
+            const u32 ngrp = take_group(s, lane);
+            if (ngrp * 32 + lane < U.len) ny = rows[U.start + ngrp * 32 + lane];
             const u32 nz = __ballot_sync(0xffffffffu, deg != 0);
             if (nz) {
                 if (deg) {
@@ -163,101 +187,142 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                 const u32 incl = warp_inclusive_sum(deg);
                 const u32 pre = incl - deg;
                 const u32 total = __shfl_sync(0xffffffffu, incl, 31);
-                const u32 le = lane == 31 ? ~0u : (2u << lane) - 1;  // positions <= lane
                 int base = -1;  // last row started before the window
-                for (u32 i0 = 0; i0 < total; i0 += 32) {
+                // edge-target address of this lane's word of window i0
+                auto addr = [&](u32 i0) -> u32 {
                     const u32 st = (deg && pre >= i0 && pre < i0 + 32) ? 1u << (pre - i0) : 0u;
                     const u32 starts = __reduce_or_sync(0xffffffffu, st);
                     const int o = base + __popc(starts & le);
                     base += __popc(starts);
                     const u32 ob = __shfl_sync(0xffffffffu, beg, o);
                     const u32 op = __shfl_sync(0xffffffffu, pre, o);
-                    const u32 i = i0 + lane;
-                    if (i < total) {
-                        const u32 w = __ldg(val + ob + (i - op));
-                        atomicOr(&row[w >> 5], 1u << (w & 31));
+                    return ob + (i0 + lane - op);
+                };
+                const u32 a0 = addr(0);  // warp-collective: every lane calls it
+                u32 w = lane < total ? __ldg(val + a0) : 0u;
+                for (u32 i0 = 0; i0 < total; i0 += 32) {
+                    const bool have = i0 + lane < total;
+                    u32 wn = 0;
+                    if (i0 + 32 < total) {
+                        const u32 a = addr(i0 + 32);
+                        if (i0 + 32 + lane < total) wn = __ldg(val + a);
                     }
+                    if (have) {
+                        const u32 old = atomicOr(&row[w >> 5], 1u << (w & 31));
+                        if (old == 0) atomicOr(&summ[w >> 10], 1u << ((w >> 5) & 31));
+                    }
+                    w = wn;
                 }
             }
+            grp = ngrp;
         }
-        __syncthreads();
-        // ---- fold the row into M: new bits = row & ~M ----
+        __syncthreads();  // (2) the row is complete
+        // ---- fold the touched words into M: new bits = row & ~M ----
         // Every new bit counts in |delta|; only targets with out-edges become
-        // rows of the next delta (the others can join nothing).
-        const u32 lim = words;  // the whole row, in order: coalesced atomics on M
+        // rows of the next delta. Warp w takes summary chunks w, w + UW, ...
         const u64 mrow = (u64) U.x * stride;
-        u64 cnt = 0;  // (new bits << 32) | new rows
-        for (u32 q0 = 0; q0 < lim; q0 += UT * 4) {
-            u32 kk[4], v[4], old[4];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const u32 q = q0 + c * UT + tid;
-                kk[c] = q;
-                v[c] = q < lim ? row[kk[c]] : 0u;
-            }
-#pragma unroll
-            for (int c = 0; c < 4; ++c) old[c] = v[c] ? atomicOr(&m[mrow + kk[c]], v[c]) : ~0u;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                if (v[c]) {
-                    const u32 f = v[c] & ~old[c];
-                    const u32 fr = f ? f & __ldg(hasout + kk[c]) : 0u;
-                    row[kk[c]] = fr;
-                    cnt += ((u64) __popc(f) << 32) | __popc(fr);
+        u32 nrows_w = 0, nbits_w = 0;
+        for (u32 c = warp; c < nchunks; c += UW) {
+            const u32 sw0 = c * SCHUNK;
+            const u32 sv = (lane < SCHUNK && sw0 + lane < swords) ? summ[sw0 + lane] : 0u;
+            u32 todo = __ballot_sync(0xffffffffu, sv != 0);
+            while (todo) {
+                // up to two summary words at once: both matrix atomics in flight
+                const u32 j0 = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const u32 j1 = todo ? __ffs(todo) - 1 : 32u;
+                if (todo) todo &= todo - 1;
+                const u32 s0 = __shfl_sync(0xffffffffu, sv, j0);
+                const u32 s1 = __shfl_sync(0xffffffffu, sv, j1 & 31);
+                const bool a0 = (s0 >> lane) & 1, a1 = j1 < 32 && ((s1 >> lane) & 1);
+                const u32 k0 = (sw0 + j0) * 32 + lane, k1 = (sw0 + (j1 & 31)) * 32 + lane;
+                const u32 v0 = a0 ? row[k0] : 0u, v1 = a1 ? row[k1] : 0u;
+                const u32 o0 = a0 ? atomicOr(&m[mrow + k0], v0) : ~0u;
+                const u32 o1 = a1 ? atomicOr(&m[mrow + k1], v1) : ~0u;
+                const u32 h0 = a0 ? __ldg(hasout + k0) : 0u, h1 = a1 ? __ldg(hasout + k1) : 0u;
+                const u32 f0 = v0 & ~o0, f1 = v1 & ~o1;
+                const u32 r0 = f0 & h0, r1 = f1 & h1;
+                if (a0) row[k0] = r0;
+                if (a1) row[k1] = r1;
+                nbits_w += __popc(f0) + __popc(f1);
+                nrows_w += __popc(r0) + __popc(r1);
+                const u32 m0 = __ballot_sync(0xffffffffu, r0 != 0);
+                const u32 m1 = __ballot_sync(0xffffffffu, r1 != 0);
+                if (lane == 0) {
+                    summ[sw0 + j0] = m0;  // summary now marks words with new rows
+                    if (j1 < 32) summ[sw0 + j1] = m1;
                 }
             }
         }
-        u64 both;
-        const u32 pos = (u32) block_exclusive_sum<UT / 32>(cnt, s.scratch64, &both);
-        const u32 total = (u32) both;  // new rows of the unit
+        nrows_w = warp_sum(nrows_w);
+        nbits_w = warp_sum(nbits_w);
+        if (lane == 0) {
+            s.wrows[warp] = nrows_w;
+            s.wbits[warp] = nbits_w;
+        }
+        __syncthreads();  // (3) per-warp counts
+        const u32 cw = lane < UW ? s.wrows[lane] : 0u;
+        const u32 bw = lane < UW ? s.wbits[lane] : 0u;
+        const u32 cinc = warp_inclusive_sum(cw);
+        const u32 total = __shfl_sync(0xffffffffu, cinc, 31);
+        const u32 before = __shfl_sync(0xffffffffu, cinc - cw, warp);  // new rows of lower warps
+        const u32 fresh = warp_sum(bw);
         if (tid == 0) {
             s.obase = total ? atomicAdd(&ctr->words, (unsigned long long) total) : 0ull;
-            if (both >> 32) atomicAdd(&ctr->fresh, both >> 32);
+            if (fresh) atomicAdd(&ctr->fresh, (unsigned long long) fresh);
         }
-        __syncthreads();
-        // ---- emit the new tuples (targets of x), clear the row ----
+        __syncthreads();  // (4) the unit's place in the next delta
         const u64 obase = s.obase;
-        u64 p = obase + pos;
+        // ---- emit the new rows (targets of x) and clear the row ----
+        // New bits are sparse within a word, so each lane walks its own word.
+        u64 p = obase + before;
         u64 dsum = 0;
-        for (u32 q0 = 0; q0 < lim; q0 += UT * 4) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const u32 q = q0 + c * UT + tid;
-                if (q >= lim) continue;
-                const u32 k = q;
-                u32 f = row[k];
-                if (!f) continue;
-                row[k] = 0;
-                while (f) {
-                    const u32 b = __ffs(f) - 1;
-                    f &= f - 1;
-                    const u32 wv = k * 32 + b;
-                    if (p < out_cap) out[p] = wv;
-                    else atomicOr(err, DL_DEVERR_CAPACITY);  // more new tuples than join words: reported
-                    ++p;
-                    dsum += __ldg(off + wv + 1) - __ldg(off + wv);
+        for (u32 c = warp; c < nchunks; c += UW) {
+            const u32 sw0 = c * SCHUNK;
+            const u32 sv = (lane < SCHUNK && sw0 + lane < swords) ? summ[sw0 + lane] : 0u;
+            if (lane < SCHUNK && sw0 + lane < swords && sv) summ[sw0 + lane] = 0;
+            u32 todo = __ballot_sync(0xffffffffu, sv != 0);
+            while (todo) {
+                const u32 j = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const u32 sj = __shfl_sync(0xffffffffu, sv, j);
+                const u32 kb = (sw0 + j) * 32;
+                u32 fr = 0;
+                if ((sj >> lane) & 1) {
+                    fr = row[kb + lane];
+                    row[kb + lane] = 0;
                 }
+                const u32 cnt = __popc(fr);
+                const u32 incl = warp_inclusive_sum(cnt);
+                u64 q = p + (incl - cnt);
+                while (fr) {
+                    const u32 t = (kb + lane) * 32 + (__ffs(fr) - 1);
+                    fr &= fr - 1;
+                    if (q < out_cap) out[q] = t;
+                    else atomicOr(err, DL_DEVERR_CAPACITY);  // more new tuples than join words: reported
+                    ++q;
+                    dsum += __ldg(off + t + 1) - __ldg(off + t);
+                }
+                p += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
-        u64 dtot;
-        block_exclusive_sum<UT / 32>(dsum, s.scratch64, &dtot);
-        if (total) {
+        // rows of the row words untouched by the fold are already zero; the
+        // touched ones were zeroed in the fold (no new rows) or just now
+        dsum = warp_sum(dsum);
+        if (lane == 0 && dsum) atomicAdd(&ctr->join, (unsigned long long) dsum);
+        if (warp == 0 && total) {
             const u64 nsub = (total + unit_rows - 1) / unit_rows;
-            if (tid == 0) {
-                if (dtot) atomicAdd(&ctr->join, (unsigned long long) dtot);
-                s.obase = atomicAdd(&ctr->units, (unsigned long long) nsub);
-            }
-            __syncthreads();
-            const u64 ub = s.obase;
-            for (u64 i = tid; i < nsub; i += UT) {
+            u64 ub = 0;
+            if (lane == 0) ub = atomicAdd(&ctr->units, (unsigned long long) nsub);
+            ub = __shfl_sync(0xffffffffu, ub, 0);
+            for (u64 i = lane; i < nsub; i += 32) {
                 if (ub + i < uout_cap)
                     uout[ub + i] = Unit{U.x, (u32) min(unit_rows, total - i * unit_rows), obase + i * unit_rows};
                 else
                     atomicOr(err, DL_DEVERR_CAPACITY);
             }
         }
-        if (tid == 0) s.next_group = 0;
-        __syncthreads();
+        if (tid == 0) s.next_group = 0;  // read again only after barrier (1)
     }
 }
 
@@ -281,64 +346,89 @@ __device__ __forceinline__ u32 transpose32(u32 v, u32 lane) {
     return v;
 }
 
-// t = transpose of a (both n rows of `stride` words). A tile is 512 source
-// rows x 512 columns: 64 bytes read from every source row and 64 bytes
-// written to every target row. One warp per 32 source rows.
-constexpr int TR_SMEM = 2 * TR_ROWS * (TR_WORDS + 1) * 4;
-__global__ void __launch_bounds__(TR_ROWS) bitmat_transpose_kernel(const u32 *__restrict__ a, u32 *__restrict__ t,
-                                                                   u64 n, u64 stride) {
+__device__ __forceinline__ void cp_async4(u32 *dst, const u32 *src) {
+    const unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// t = transpose of a (both n rows of `stride` words), and counts[w] += set
+// bits of target row w. A tile is 512 source rows x 512 columns: 64 bytes
+// read from every source row and 64 bytes written to every target row. CTA
+// (c, g) walks the tiles of column block c (targets 512 c ...) for source
+// blocks g, g + G, ...; the next tile is copied into shared memory (cp.async,
+// two buffers) while the current one is transposed and stored. Thread i keeps
+// the popcount of target row 512 c + i over its tiles and adds it to counts
+// once at the end (G atomics per row).
+constexpr int TR_PAD = TR_WORDS + 1;
+constexpr int TR_SMEM = 3 * TR_ROWS * TR_PAD * 4;  // two input tiles + the transposed tile
+__global__ void __launch_bounds__(TR_ROWS, 2) bitmat_transpose_count_kernel(const u32 *__restrict__ a,
+                                                                            u32 *__restrict__ t, u64 n, u64 stride,
+                                                                            unsigned long long *__restrict__ counts) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    u32(*in)[TR_WORDS + 1] = reinterpret_cast<u32(*)[TR_WORDS + 1]>(smem_raw);
-    u32(*outw)[TR_ROWS / 32 + 1] = reinterpret_cast<u32(*)[TR_ROWS / 32 + 1]>(smem_raw + TR_ROWS * (TR_WORDS + 1) * 4);
+    u32(*in)[TR_ROWS][TR_PAD] = reinterpret_cast<u32(*)[TR_ROWS][TR_PAD]>(smem_raw);
+    u32(*outw)[TR_ROWS / 32 + 1] = reinterpret_cast<u32(*)[TR_ROWS / 32 + 1]>(smem_raw + 2 * TR_ROWS * TR_PAD * 4);
     static_assert(TR_WORDS * 32 == TR_ROWS && TR_ROWS / 32 == TR_WORDS, "square tile: 512 x 512 bits");
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const u64 x0 = (u64) blockIdx.y * TR_ROWS;
-    const u64 c0 = (u64) blockIdx.x * TR_WORDS;
-    u32 v[TR_WORDS];  // all of a thread's loads in flight before the first store
+    const u64 c0 = (u64) blockIdx.x * TR_WORDS;  // first column word of the block
+    const u64 nblocks = (n + TR_ROWS - 1) / TR_ROWS;
+    auto issue = [&](u64 b, int buf) {  // tile (b, c) -> in[buf]
+        const u64 x0 = b * TR_ROWS;
 #pragma unroll
-    for (u32 j = 0; j < TR_WORDS; ++j) {
-        const u32 i = tid + j * TR_ROWS, r = i / TR_WORDS, c = i % TR_WORDS;
-        const u64 x = x0 + r, col = c0 + c;
-        v[j] = (x < n && col < stride) ? __ldcs(a + x * stride + col) : 0u;
-    }
-#pragma unroll
-    for (u32 j = 0; j < TR_WORDS; ++j) {
-        const u32 i = tid + j * TR_ROWS;
-        in[i / TR_WORDS][i % TR_WORDS] = v[j];
-    }
-    __syncthreads();
+        for (u32 j = 0; j < TR_WORDS; ++j) {
+            const u32 i = tid + j * TR_ROWS, r = i / TR_WORDS, c = i % TR_WORDS;
+            const u64 x = x0 + r, col = c0 + c;
+            if (x < n && col < stride) cp_async4(&in[buf][r][c], a + x * stride + col);
+            else in[buf][r][c] = 0u;
+        }
+    };
+    u32 cnt = 0;  // set bits of target row c0 * 32 + tid in this CTA's tiles
+    u64 b = blockIdx.y;
+    int buf = 0;
+    if (b < nblocks) issue(b, 0);
+    cp_async_commit();
+    for (; b < nblocks; b += gridDim.y, buf ^= 1) {
+        // in[buf ^ 1] was last read by the previous tile's transpose, which
+        // every thread finished before the barrier ahead of its stores
+        if (b + gridDim.y < nblocks) issue(b + gridDim.y, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait_prev();  // this thread's copies of tile b have landed
+        __syncthreads();       // everyone's have
 #pragma unroll 4
-    for (u32 c = 0; c < TR_WORDS; ++c) outw[c * 32 + lane][warp] = transpose32(in[warp * 32 + lane][c], lane);
-    __syncthreads();
-    for (u32 i = tid; i < TR_WORDS * 32 * (TR_ROWS / 32); i += TR_ROWS) {
-        const u32 r = i / (TR_ROWS / 32), xw = i % (TR_ROWS / 32);
-        const u64 w = c0 * 32 + r, col = x0 / 32 + xw;
-        if (w < n && col < stride) t[w * stride + col] = outw[r][xw];
+        for (u32 c = 0; c < TR_WORDS; ++c)
+            outw[c * 32 + lane][warp] = transpose32(in[buf][warp * 32 + lane][c], lane);
+        __syncthreads();
+#pragma unroll
+        for (u32 xw = 0; xw < TR_ROWS / 32; ++xw) cnt += __popc(outw[tid][xw]);
+        const u64 x0 = b * TR_ROWS;
+#pragma unroll 4
+        for (u32 j = 0; j < TR_WORDS; ++j) {
+            const u32 i = tid + j * TR_ROWS;
+            const u32 r = i / (TR_ROWS / 32), xw = i % (TR_ROWS / 32);
+            const u64 w = c0 * 32 + r, col = x0 / 32 + xw;
+            if (w < n && col < stride) t[w * stride + col] = outw[r][xw];
+        }
+        // outw is rewritten only after the next iteration's first barrier
     }
+    const u64 w = c0 * 32 + tid;
+    if (w < n && cnt) atomicAdd(counts + w, (unsigned long long) cnt);
 }
 
-// counts[w] = set bits among the first `words` words of row w (warp per row).
-__global__ void bitmat_row_count_kernel(const u32 *__restrict__ t, u64 n, u64 stride, u64 words, u64 *__restrict__ counts) {
-    const u32 lane = threadIdx.x & 31;
-    const u64 warps = (u64) gridDim.x * (blockDim.x / 32);
-    for (u64 w = ((u64) blockIdx.x * blockDim.x + threadIdx.x) / 32; w < n; w += warps) {
-        const u32 *row = t + w * stride;
-        u32 c = 0;
-        for (u64 k = lane; k < words; k += 32) c += __popc(__ldcs(row + k));
-        c = warp_sum(c);
-        if (lane == 0) counts[w] = c;
-    }
-}
-
-// Row w of t -> words (w << bits) | x for its set bits x, ascending, from
-// out[first[w]] on (warp per row). A lane takes 4 consecutive words per step
-// (one 16-byte load); a step's words are staged in shared memory and leave
-// with consecutive stores unless there are more than EX_STAGE of them.
+// Row w of t -> result rows (ids[x], ids[w]) for its set bits x, ascending,
+// from out[first[w]] on: the reference's TC file order (x, z) sorted by
+// (z, x). One warp per row; a lane takes 4 consecutive words per step (one
+// 16-byte load, the next one in flight); a step's rows are staged in shared
+// memory and leave with consecutive stores unless there are more than
+// EX_STAGE of them. (Result words are sparse -- C1 averages well under one
+// set bit per non-zero word -- so each lane walks its own words' bits.)
 constexpr int EX_THREADS = 256;
 constexpr int EX_STAGE = 256;
-__global__ void __launch_bounds__(EX_THREADS) bitmat_extract_kernel(const u32 *__restrict__ t, u64 n, u64 stride,
-                                                                    u64 words, int bits, const u64 *__restrict__ first,
-                                                                    u64 *__restrict__ out) {
+__global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u32 *__restrict__ t, u64 n,
+                                                                         u64 stride, u64 words,
+                                                                         const u64 *__restrict__ first,
+                                                                         const int32_t *__restrict__ ids,
+                                                                         u64 *__restrict__ out) {
     __shared__ u64 stage[EX_THREADS / 32][EX_STAGE];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     u64 *st = stage[warp];
@@ -346,7 +436,7 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_kernel(const u32 *_
     for (u64 w = (u64) blockIdx.x * (EX_THREADS / 32) + warp; w < n; w += warps) {
         const u32 *row = t + w * stride;
         u64 pos = first[w];
-        const u64 hi = w << bits;
+        const u64 hi = (u64) (u32) ids[w] << 32;  // (x id, z id) as one little-endian 8-byte row
         // stride is a multiple of 32 words: a lane's vector stays in the row
         uint4 nxt = make_uint4(0, 0, 0, 0);
         if ((u64) lane * 4 < words) nxt = __ldcs(reinterpret_cast<const uint4 *>(row + lane * 4));
@@ -367,7 +457,8 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_kernel(const u32 *_
             if (sum <= EX_STAGE) {
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
-                    for (u32 b = v[c]; b; b &= b - 1) st[p++] = hi | ((k + c) * 32 + (u64) (__ffs(b) - 1));
+                    for (u32 b = v[c]; b; b &= b - 1)
+                        st[p++] = hi | (u32) __ldg(ids + (k + c) * 32 + (__ffs(b) - 1));
                 __syncwarp();
                 for (u32 i = lane; i < sum; i += 32) out[pos + i] = st[i];
                 __syncwarp();
@@ -375,7 +466,8 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_kernel(const u32 *_
                 u64 q2 = pos + p;
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
-                    for (u32 b = v[c]; b; b &= b - 1) out[q2++] = hi | ((k + c) * 32 + (u64) (__ffs(b) - 1));
+                    for (u32 b = v[c]; b; b &= b - 1)
+                        out[q2++] = hi | (u32) __ldg(ids + (k + c) * 32 + (__ffs(b) - 1));
             }
             pos += sum;
         }
@@ -433,7 +525,7 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
     const u64 stride = bitmat_stride(n);
     const u64 unit_rows = std::max<u64>(1, ctx.tune.bitmap_unit_rows);
     const u64 words_used = (n + 31) / 32;
-    const size_t smem = sizeof(UnitSmem) + words_used * 4 + 16;
+    const size_t smem = sizeof(UnitSmem) + (words_used + (words_used + 31) / 32) * 4 + 16;
     if (smem > 227 * 1024) throw Error(DL_ERR_OUT_OF_MEMORY, "bit-matrix rows of " + std::to_string(n) +
                                                               " nodes do not fit in shared memory");
     DevBuf &M = ws.bitmat[0];
@@ -521,32 +613,56 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
     }
     pt.mark(PH_FINAL);
-    // full -> sorted (w << bits) | x words in ws.full[0]
-    ctx.reserve(ws.full[0], std::max<u64>(nfull, 1) * 8);
+    // full -> its transpose (row = target) and per-target counts; the result
+    // rows are extracted from it when they are copied out (bitmat_extract_rows)
     if (nfull) {
         DevBuf &T = ws.bitmat[1];
         ctx.reserve(T, bitmat_bytes(n));
-        const dim3 tg((unsigned) (stride / TR_WORDS), (unsigned) ((n + TR_ROWS - 1) / TR_ROWS));
-        DL_CUDA(cudaFuncSetAttribute(bitmat_transpose_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TR_SMEM));
-        DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 2.0 * bitmat_bytes(n),
-                  bitmat_transpose_kernel<<<tg, TR_ROWS, TR_SMEM, ctx.stream>>>(m, T.as<u32>(), n, stride));
         ctx.reserve(ws.offsets, (n + 1) * 8);
         u64 *counts = ws.offsets.as<u64>();
+        DL_CUDA(cudaMemsetAsync(counts, 0, n * 8, ctx.stream));
+        DL_CUDA(cudaFuncSetAttribute(bitmat_transpose_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TR_SMEM));
+        int tr_per_sm = 0;
+        DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, bitmat_transpose_count_kernel, TR_ROWS,
+                                                              TR_SMEM));
+        const u64 xblocks = stride / TR_WORDS, nblocks = (n + TR_ROWS - 1) / TR_ROWS;
+        const u64 resident_tr = (u64) ctx.sm_count * std::max(tr_per_sm, 1);
+        const u64 gy = std::min<u64>(nblocks, std::max<u64>(1, (8 * resident_tr + xblocks - 1) / xblocks));
+        const dim3 tg((unsigned) xblocks, (unsigned) gy);
+        DL_LAUNCH(ctx, K_BITMAP_TRANSPOSE, 2.0 * bitmat_bytes(n),
+                  bitmat_transpose_count_kernel<<<tg, TR_ROWS, TR_SMEM, ctx.stream>>>(
+                      m, T.as<u32>(), n, stride, reinterpret_cast<unsigned long long *>(counts)));
         ctx.reserve(ws.w0, (n + 1) * 8);
         u64 *first = ws.w0.as<u64>();
-        const unsigned rg = grid_for(n * 32, T256, ctx, 8);
-        DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 4.0 * n * words_used,
-                  bitmat_row_count_kernel<<<rg, T256, 0, ctx.stream>>>(T.as<u32>(), n, stride, words_used, counts));
         const u64 total = exclusive_scan(ctx, counts, n, first);
         if (total != nfull)
             throw Error(DL_ERR_INTERNAL, "bit matrix holds " + std::to_string(total) + " tuples, expected " +
                                              std::to_string(nfull));
-        DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 4.0 * n * words_used + 8.0 * nfull,
-                  bitmat_extract_kernel<<<grid_for(n * 32, EX_THREADS, ctx, 8), EX_THREADS, 0, ctx.stream>>>(
-                      T.as<u32>(), n, stride, words_used, g.bits, first, ws.full[0].as<u64>()));
+        r.bm_t = T;
+        T = DevBuf();
+        r.bm_first = ws.w0;
+        ws.w0 = DevBuf();
+        r.bm_n = n;
+        r.bm_stride = stride;
+        r.bm_words = words_used;
     }
+    r.from_bitmat = true;
     return nfull;
 }
 
 }  // namespace detail
+
+// The result rows of a bit-matrix TC run, written straight from the stored
+// transpose into `out` (device memory): (x, z) rows ordered by (z, x).
+void bitmat_extract_rows(Context &ctx, const Run &r, int32_t *out) {
+    using namespace detail;
+    if (r.info.output_rows == 0) return;
+    const u64 n = r.bm_n;
+    DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 4.0 * n * r.bm_words + 8.0 * (double) r.info.output_rows,
+              bitmat_extract_rows_kernel<<<grid_for(n * 32, EX_THREADS, ctx, 8), EX_THREADS, 0, ctx.stream>>>(
+                  r.bm_t.as<u32>(), n, r.bm_stride, r.bm_words, r.bm_first.as<u64>(), r.ids.as<int32_t>(),
+                  reinterpret_cast<u64 *>(out)));
+}
+
 }  // namespace dl

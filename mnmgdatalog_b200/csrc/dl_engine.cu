@@ -467,7 +467,7 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, n, 2 * g.bits, ne);
         build_csr(ctx, e, ne, g);
         if (bitmat_choose(ctx, opt, g.n_ids)) {
-            nfull = tc_bitmap_fixpoint(ctx, r, g, e, ne, opt, pt);  // result in ws.full[0]
+            nfull = tc_bitmap_fixpoint(ctx, r, g, e, ne, opt, pt);  // result: the transpose, in r
             cur = 0;
         } else {
             u64 nd;
@@ -500,9 +500,11 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     DL_CUDA(cudaEventRecord(ev.b, ctx.stream));
     pt.mark(PH_FINAL);
     adopt_ids(ctx, r, g);
-    r.words = ws.full[cur];
-    ws.full[cur] = DevBuf();
-    r.n_words = nfull;
+    if (!r.from_bitmat) {
+        r.words = ws.full[cur];
+        ws.full[cur] = DevBuf();
+        r.n_words = nfull;
+    }
     r.info.output_rows = r.info.output_tuples = (i64) nfull;
     finish_info(r, ctx, ev.a, ev.b, pt);
 }
@@ -810,7 +812,9 @@ void run_copy_output(const Run &r, int32_t *dst, u64 capacity, bool dst_on_devic
         tmp = stage.as<int32_t>();
     }
     const int32_t *ids = r.ids.as<int32_t>();
-    if (r.program == DL_PROGRAM_WCC) {
+    if (r.from_bitmat) {
+        bitmat_extract_rows(ctx, r, tmp);
+    } else if (r.program == DL_PROGRAM_WCC) {
         DL_LAUNCH(ctx, K_PREP, 0, unpack_components_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.aux.as<u32>(), n, ids, tmp));
     } else if (r.program == DL_PROGRAM_SG) {
         DL_LAUNCH(ctx, K_PREP, 0, unpack_rows_kernel<true><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.words.as<u64>(), n, r.bits, ids, tmp));
@@ -847,6 +851,8 @@ void run_destroy(Run *r) {
         r->ctx->give_back(r->ids);
         r->ctx->give_back(r->aux);
         r->ctx->give_back(r->labels);
+        r->ctx->give_back(r->bm_t);
+        r->ctx->give_back(r->bm_first);
     }
     delete r;
 }

@@ -20,11 +20,18 @@ struct Run {
     DevBuf aux;               // WCC: component ranks, ascending
     u64 n_aux = 0;
     DevBuf labels;            // WCC: label rank of every node
+    // TC on the bit matrix: the result stays as the matrix's transpose (row =
+    // path target) and each row's first output position; rows are extracted
+    // when they are copied out
+    bool from_bitmat = false;
+    DevBuf bm_t, bm_first;
+    u64 bm_n = 0, bm_stride = 0, bm_words = 0;
 };
 
 Run *run_program(Context &ctx, int program, const int32_t *rows, u64 n, bool on_device, const dl_options &opt);
 void run_copy_output(const Run &r, int32_t *dst, u64 capacity, bool dst_on_device);
 void run_copy_labels(const Run &r, int32_t *node_ids, int32_t *labels, u64 capacity);
 void run_destroy(Run *r);
+void bitmat_extract_rows(Context &ctx, const Run &r, int32_t *out);
 
 }  // namespace dl

@@ -51,6 +51,7 @@ struct Error : std::runtime_error {
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
+    bool fixed = false;  // a slice of memory the buffer does not own: never grown or freed
     void reserve(size_t bytes, bool zero = false);
     void release();
     template <typename T>
@@ -77,7 +78,8 @@ enum KernelId : int {
     K_HASH_INSERT,     // hash-set dedup: 8 B read + 32 B probe sector per word, 40 B per new word
     K_BITMAP_EXPAND,   // bit-matrix TC step: 4 B per delta row in and out + 16 B per unit in and out +
                        // 4 B edge target per join word
-    K_BITMAP_EXTRACT,  // bit-matrix transpose, row counts, scan and word extraction of the result
+    K_BITMAP_TRANSPOSE,  // bit-matrix transpose with per-target counts: 2 x matrix bytes
+    K_BITMAP_EXTRACT,  // result rows from the transposed matrix: matrix read + 8 B per result row (+ count scan)
     // host-side costs, counted with or without profiling (seconds = host wall time)
     K_HOST_MALLOC,     // cudaMalloc of a buffer that had to grow (bytes = size)
     K_HOST_FREE,       // cudaFree of a cached buffer dropped from the cache
@@ -135,6 +137,7 @@ struct Context {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int sm_count = 148;
+    bool no_alloc = false;          // every buffer is a fixed slice; a new allocation is an internal error
     Ctrl *ctrl = nullptr;           // device control block
     u32 epoch = 0;                  // look-back epoch of the last launch
     DevBuf lookback;                // look-back words (zeroed at allocation)
@@ -143,6 +146,7 @@ struct Context {
     DevBuf radix_part;              // per-(digit, CTA) counts and offsets of a radix pass
     DevBuf merge_splits;            // merge-path split points of a set operation
     DevBuf bucket_cursor;           // per-digit output cursors of the bucketed join emit
+    DevBuf part_cursor;             // per-destination counts and cursors of a hash partition
     u64 *host_scalars = nullptr;    // pinned mirror for small D2H reads
     Workspace ws;
     u64 run_join_total = 0, run_join_max = 0;  // join statistics of the current run
@@ -223,6 +227,13 @@ u64 unique_words(Context &ctx, const u64 *in, u64 n, u64 *out, int by_key_shift 
                  Codec codec = Codec::Raw);
 // Drops entity words whose key equals value. `out` may alias `in`.
 u64 remove_self_pairs_words(Context &ctx, const u64 *in, u64 n, u64 *out);
+
+// ---- hash partition for the multi-GPU exchange (dl_partition.cu) ------------
+constexpr u32 kMaxPartitionRanks = 4096;
+// out = rel's rows grouped by owner(key) = fmix32(key) % ranks, destination
+// 0 first (order inside a group unspecified); counts[r] = rows owned by r.
+// swap: rows leave as (value, key) and are owned by their value.
+void partition_rows(Context &ctx, const int32_t *rel, u64 n, u32 ranks, bool swap, int32_t *out, i64 *counts);
 // Drops all-ones words (the engine's "removed" marker). `out` may alias `in`.
 // `kind` is unused (reserved).
 u64 select_words(Context &ctx, const u64 *in, u64 n, u64 *out, int kind);
