@@ -14,8 +14,9 @@ independent replica (the path is one fixpoint per GPU; no collective on the
 data path); timing is on the device (CUDA events) and the max over ranks.
 
 --impl reference times the reference's own CPU program (rough/tc_mpi.cpp, built
-by oracle/Makefile into oracle/_ref/tc_mpi; one MPI rank = one core) on a
-bounded sample of the same graph family, rank 0 only.
+unmodified by oracle/Makefile into oracle/_ref/tc_mpi_fork: one MPI rank per
+host core over a fork + shared-memory MPI) on a bounded sample of the same
+graph family, rank 0 only.
 """
 from __future__ import annotations
 
@@ -38,10 +39,11 @@ sys.path.insert(0, ROOT)
 METRIC = "derived tuples/s per fixpoint"
 UNIT = "tuples/s"
 L2_FLUSH_BYTES = 256 << 20
-CPU_SAMPLE_NODES = 8000      # cpu_baseline sample (~15-25 s on one core)
-REF_SAMPLE_NODES = 6000      # reference arm sample per step (~5-10 s)
+CPU_SAMPLE_NODES = 24000     # cpu_baseline sample (~10-20 s over 8-16 cores)
+REF_SAMPLE_NODES = 12000     # reference arm sample per step (a few seconds over 16 cores)
 HBM_FALLBACK_GBS = 6650.0
 TUNING_BATCH = os.path.join(ROOT, "mnmgdatalog_b200", "tuning_batch.json")
+SERVE_BUDGET = 150 * 10**9   # HBM budget of the served leg's admission
 
 
 def _env_int(k, d):
@@ -131,16 +133,22 @@ class ClockSampler:
 
 
 def run_tc_mpi_sample(nodes: int, seed: int = 0) -> dict:
-    """Time the reference CPU program on a Chung-Lu sample of `nodes` nodes."""
+    """Time the reference CPU program on a Chung-Lu sample of `nodes` nodes,
+    as one MPI rank per host core (oracle/_ref/tc_mpi_fork: the unmodified
+    rough/tc_mpi.cpp over the fork + shared-memory MPI of oracle/mpi_fork),
+    else as one rank (oracle/_ref/tc_mpi), else the oracle's restatement."""
     from mnmgdatalog_b200 import graphs
     e = graphs.chung_lu(n=nodes, m=int(round(nodes * 1_050_000 / 317_000)), seed=seed)
-    binary = os.path.join(ROOT, "oracle", "_ref", "tc_mpi")
+    forked = os.path.join(ROOT, "oracle", "_ref", "tc_mpi_fork")
+    single = os.path.join(ROOT, "oracle", "_ref", "tc_mpi")
+    binary, ranks = (forked, os.cpu_count() or 1) if os.path.exists(forked) else (single, 1)
     with tempfile.TemporaryDirectory() as td:
         inp = os.path.join(td, "sample.bin")
         e.astype("<i4").tofile(inp)
         if os.path.exists(binary):
             t0 = time.perf_counter()
-            r = subprocess.run([binary, inp], capture_output=True, text=True, timeout=600, check=True)
+            r = subprocess.run([binary, inp], capture_output=True, text=True, timeout=600, check=True,
+                               env=dict(os.environ, MPI_FORK_RANKS=str(ranks)))
             wall = time.perf_counter() - t0
             row = [l for l in r.stdout.splitlines() if l.startswith("|") and l[2:3].isdigit()][-1]
             cells = [c.strip().replace(",", "").replace("'", "") for c in row.strip("|").split("|")]
@@ -152,10 +160,11 @@ def run_tc_mpi_sample(nodes: int, seed: int = 0) -> dict:
             res = cpu.tc(e)
             secs = wall = time.perf_counter() - t0
             tuples = len(res.rows)
-            kind = "port"
-    return {"value": tuples / secs, "unit": UNIT, "cores": 1, "kind": kind,
+            kind, ranks = "port", 1
+    return {"value": tuples / secs, "unit": UNIT, "cores": ranks, "kind": kind,
             "sample": f"TC of Chung-Lu n={nodes} m={len(e)} gamma=2.5 (same generator, seed {seed}): "
-                      f"{tuples} tuples in {secs:.2f} s (wall {wall:.2f} s), one MPI rank",
+                      f"{tuples} tuples in {secs:.2f} s (wall {wall:.2f} s), {ranks} MPI rank(s) of "
+                      f"rough/tc_mpi.cpp, one per host core",
             "tuples": tuples, "seconds": secs}
 
 
@@ -553,7 +562,7 @@ def measure_served(eng, args, tuning=None) -> dict:
 
     # one server for all runs: its sessions and buffers stay warm, like a
     # service that has been up for a while
-    srv = serve.Server(eng, budget_bytes=150 * 10**9, keep_results=False, concurrent=True, pinned=True,
+    srv = serve.Server(eng, budget_bytes=SERVE_BUDGET, keep_results=False, concurrent=True, pinned=True,
                        tuning=tuning)
     try:
         srv.serve([serve.Request(r.id, r.program, r.edges) for r in reqs[:120]])  # warm-up

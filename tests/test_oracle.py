@@ -77,3 +77,31 @@ def test_tc_closure_brute_force_small():
                     changed = True
         want = sorted(((x, z) for x in nodes for z in reach[x]), key=lambda t: (t[1], t[0]))
         assert cpu.tc(e).rows.tolist() == [list(t) for t in want]
+
+
+@pytest.mark.parametrize("ranks", [1, 3, 4])
+@pytest.mark.parametrize("fname", ["data_7035.bin", "synth_dag_c0.bin"])
+def test_reference_cpu_program_on_forked_ranks(expected, tmp_path, fname, ranks):
+    """The reference's CPU program rough/tc_mpi.cpp as several MPI ranks on
+    the host (oracle/_ref/tc_mpi_fork, the CPU baseline): the same closure as
+    the oracle's one-rank answer. With several ranks the file holds each
+    rank's partition in rank order, so the rows are compared as a set."""
+    import os
+    import subprocess
+
+    from conftest import ROOT
+    binary = os.path.join(ROOT, "oracle", "_ref", "tc_mpi_fork")
+    if not os.path.exists(binary):
+        pytest.skip("oracle/_ref/tc_mpi_fork not built (needs the reference sources)")
+    inp = tmp_path / fname
+    load_input(fname).astype("<i4").tofile(inp)
+    r = subprocess.run([binary, str(inp)], capture_output=True, text=True, timeout=300,
+                       env=dict(os.environ, MPI_FORK_RANKS=str(ranks)))
+    assert r.returncode == 0, r.stderr
+    row = [l for l in r.stdout.splitlines() if l.startswith("|") and l[2:3].isdigit()][-1]
+    cells = [c.strip().replace(",", "").replace("'", "") for c in row.strip("|").split("|")]
+    rec = expected["inputs"][fname]["tc"]
+    assert (int(cells[1]), int(cells[2]), int(cells[3])) == (ranks, rec["iterations"], rec["rows_count"])
+    rows = np.fromfile(str(inp) + "_tc.bin", dtype="<i4").reshape(-1, 2)
+    rows = rows[np.lexsort((rows[:, 0], rows[:, 1]))]  # the one-rank file order: (x, z) by (z, x)
+    assert sha_rows(rows) == rec["rows_sha256"]
