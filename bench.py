@@ -349,6 +349,14 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
             sg = {"error": f"{type(exc).__name__}: {exc}"}
         release(eng, torch)
 
+    sj = None
+    if args.single_join_leg and world == 1:
+        try:
+            sj = measure_single_join(eng, args, dev, flush)
+        except Exception as exc:  # reported in the line, never hidden
+            sj = {"error": f"{type(exc).__name__}: {exc}"}
+        release(eng, torch)
+
     batched = served = None
     if args.batch_instances > 0:
         try:
@@ -386,7 +394,7 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
                 "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
                 "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clk, "kernels": kernels, "host": host_costs,
-                "step_ms": [round(x, 3) for x in ms], "reference_gpu": ref_gpu, "sg": sg,
+                "step_ms": [round(x, 3) for x in ms], "reference_gpu": ref_gpu, "sg": sg, "single_join": sj,
                 "batched": batched, "served": served}
         print(json.dumps(line))
     eng.close()
@@ -401,6 +409,45 @@ def load_fixture(name: str) -> np.ndarray:
     with gzip.open(os.path.join(ROOT, "tests", "golden", "data", name + ".gz"), "rb") as f:
         raw = f.read()
     return np.frombuffer(raw, dtype="<i4")[: (len(raw) // 8) * 2].reshape(-1, 2).copy()
+
+
+SINGLE_JOIN = (10_000_001, 100_000, 1_037_050_773, "drawing/charts/single_join_strong (copy).csv:2")
+
+
+def measure_single_join(eng, args, dev, flush) -> dict:
+    """single_join's strong-scaling input on one GPU: 10,000,001 rows of
+    glibc srand(1)/rand() values in [1, 100,000] (the reference published
+    1,037,050,773 output rows, 1.78 s on an A100), timed like the main leg,
+    with the reference's own GPU program on the same rows."""
+    import torch
+
+    from mnmgdatalog_b200 import generate_rows
+    rows, rng, pub, cite = SINGLE_JOIN
+    data = generate_rows(rows, rng, 1)
+    ref = None
+    if not args.no_reference_gpu:
+        binary = os.path.join(ROOT, "oracle", "_ref", "single_join.out")
+        if os.path.exists(binary):
+            t0 = time.perf_counter()
+            r = subprocess.run([binary, str(rows), "0", "0", str(rng)], capture_output=True, text=True, timeout=600)
+            wall = time.perf_counter() - t0
+            if r.returncode == 0:
+                csv = [l for l in r.stdout.splitlines() if l and l[0].isdigit()][-1].split(",")
+                ref = {"program": f"oracle/_ref/single_join.out {rows} 0 0 {rng} (reference single_join.cu, "
+                                  "unmodified, one MPI rank)", "tuples": int(csv[3]), "total_s": float(csv[4]),
+                       "wall_s": round(wall, 2)}
+            else:
+                ref = {"error": f"exit {r.returncode}: {r.stderr[-300:]}"}
+    d = torch.from_numpy(data).to(dev)
+    steps = max(1, min(args.steps, 3))
+    ms, res, prof = timed_fixpoints(eng, "single_join", d, steps, 1, "auto", dev, 1, lambda: None, flush)
+    roofline, kernels, _, launches = roofline_of(prof, sum(ms) / 1e3)
+    return {"workload": f"single_join, {rows} rows, values in [1, {rng}] (the reference's strong-scaling input; "
+                        f"published {pub} output rows, {cite})",
+            "value": res.output_tuples * steps / (sum(ms) / 1e3), "unit": UNIT, "steps": steps,
+            "ms_per_step": sum(ms) / steps, "tuples": int(res.output_tuples),
+            "matches_published": bool(res.output_tuples == pub), "roofline": roofline, "kernels": kernels,
+            "gpu_launches": launches, "reference_gpu": ref}
 
 
 def measure_sg_dataset(eng, args, dev, flush) -> dict:
@@ -613,6 +660,8 @@ def main(argv=None) -> int:
                     help="how TC removes known tuples (same results)")
     ap.add_argument("--no-sg-leg", dest="sg_leg", action="store_false",
                     help="skip the SG leg on the reference's fe_body input")
+    ap.add_argument("--no-single-join-leg", dest="single_join_leg", action="store_false",
+                    help="skip the single_join leg (10M rows, the reference's strong-scaling input)")
     ap.add_argument("--batch-instances", type=int, default=1024, help="batched form instances (0: skip)")
     ap.add_argument("--autotune", action="store_true",
                     help="re-run the autotuner for the batched leg instead of the committed knobs")

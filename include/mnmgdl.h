@@ -104,7 +104,8 @@ typedef struct dl_run_info {
     int64_t output_rows;         /* rows of the program's output file */
     int64_t output_tuples;       /* TC/SG/single_join: |result|; WCC: # components */
     int64_t largest_component;   /* WCC only */
-    int64_t nodes;               /* distinct node ids in the input */
+    int64_t nodes;               /* node ranks of the run: the distinct node ids of the input (TC on the
+                                    bit-matrix path over a dense id range: every id of that range) */
     double seconds_total;        /* device time, H2D of the input through the last iteration */
     double seconds_init;         /* phase times (phase_timing = 1), reference CSV columns */
     double seconds_join;
@@ -143,7 +144,8 @@ typedef struct dl_tuning {
     int32_t join_first_pass;      /* TC: 1 = the join emit also does the sort's first radix pass (default), 0 = not */
     int32_t bitmap_max_gib;       /* TC dedup AUTO: largest bit matrix + transpose, GiB (0..1024, default 48; 0 = never) */
     int32_t bitmap_unit_rows;     /* bit-matrix TC: delta rows per work unit (1..16777216, default 65536) */
-    int32_t reserved[1];
+    int32_t cache_max_gib;        /* outgrown or released device buffers the context keeps for reuse, at most
+                                     this many GiB (0..1024, default 96; 0 = free them at once) */
 } dl_tuning;
 DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out);
 DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *tuning);
@@ -173,6 +175,19 @@ DL_API dl_status dl_unique_by_key_min(dl_context *ctx, dl_entity *rel, int64_t n
 /* Drop rows with key == value, order kept. */
 DL_API dl_status dl_remove_self_pairs(dl_context *ctx, dl_entity *rel, int64_t n, int64_t *n_out);
 
+/* Multi-GPU exchange, send side: out = rel's rows grouped by destination
+ * rank, rank 0's rows first; counts[r] (a host array of `ranks` entries)
+ * receives the number of rows rank r owns. owner(row) = murmur3 fmix32 of
+ * its key's unsigned 32-bit pattern, mod ranks -- the reference's
+ * get_rank / get_send_count / get_rank_data (common/kernels.cu:199-242),
+ * whose signed modulo is replaced by an unsigned one. With swap_columns != 0
+ * every row (a, b) is written as (b, a) and owned by b (the reference's
+ * reverse_entity_ar before an exchange, common/kernels.cu:313-324). The
+ * order inside a destination's rows is unspecified. 1 <= ranks <= 4096;
+ * out must not overlap rel. Returns after the rows are written. */
+DL_API dl_status dl_partition(dl_context *ctx, const dl_entity *rel, int64_t n, int32_t ranks, int32_t swap_columns,
+                              dl_entity *out, int64_t *counts);
+
 /* dl_sort_unique without any memory allocation. No counterpart in the
  * reference. For callers that cannot call cudaMalloc at sort time -- device
  * memory already owned by another allocator's pool, a fixed device footprint
@@ -181,10 +196,12 @@ DL_API dl_status dl_remove_self_pairs(dl_context *ctx, dl_entity *rel, int64_t n
  * the library (about 10 MiB on every GPU that loads it, held until the
  * process exits), so at most dl_sort_unique_noalloc_max_rows() rows
  * (1,048,576) are accepted; more is DL_ERR_INVALID_ARGUMENT. `stream` is a
- * cudaStream_t (NULL = default stream); the call returns after its GPU work
- * is done. The first call on a device looks the array up (set-up) and should
- * come before any stream capture. All calls share the array: calls whose GPU
- * work overlapped would race, so concurrent host calls are serialised. */
+ * cudaStream_t (NULL = default stream). Every call synchronises `stream`:
+ * it returns only after its own GPU work is done. The first call on a device
+ * looks the array up and clears its control words (set-up), and should come
+ * before any stream capture. All calls share the array and it keeps the last
+ * call's contents: calls whose GPU work overlapped would race, so concurrent
+ * host calls are serialised. */
 DL_API dl_status dl_sort_unique_noalloc(dl_entity *rel, int64_t n, int64_t *n_out, void *stream);
 DL_API int64_t dl_sort_unique_noalloc_max_rows(void);
 

@@ -28,7 +28,7 @@ EXPORTS = (
     "dl_context_create", "dl_context_destroy", "dl_context_synchronize", "dl_context_release_memory", "dl_free", "dl_memcpy",
     "dl_context_get_tuning", "dl_context_set_tuning",
     "dl_sort_unique", "dl_sort", "dl_set_difference", "dl_merge", "dl_diff_merge",
-    "dl_unique_by_key_min", "dl_remove_self_pairs",
+    "dl_unique_by_key_min", "dl_remove_self_pairs", "dl_partition",
     "dl_build_hash_table", "dl_hash_table_info", "dl_hash_table_destroy", "dl_join", "dl_join_sorted",
     "dl_run_program", "dl_run_tc", "dl_run_sg", "dl_run_wcc", "dl_run_single_join",
     "dl_run_get_info", "dl_run_copy_output", "dl_run_copy_deltas", "dl_run_copy_labels", "dl_run_destroy",
@@ -65,7 +65,7 @@ class dl_tuning(C.Structure):
     _fields_ = [("sort_algorithm", C.c_int32), ("sort_ranking", C.c_int32), ("sort_keys_per_thread", C.c_int32),
                 ("dense_ratio", C.c_int32), ("small_ratio", C.c_int32), ("sort_input_tma", C.c_int32),
                 ("hash_load_factor", C.c_double), ("join_first_pass", C.c_int32), ("bitmap_max_gib", C.c_int32),
-                ("bitmap_unit_rows", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("bitmap_unit_rows", C.c_int32), ("cache_max_gib", C.c_int32)]
 
 
 class dl_kernel_stat(C.Structure):
@@ -105,6 +105,7 @@ def lib():
         "dl_diff_merge": ([vp, vp, i64, vp, i64, vp, vp, pi64], C.c_int),
         "dl_unique_by_key_min": ([vp, vp, i64, pi64], C.c_int),
         "dl_remove_self_pairs": ([vp, vp, i64, pi64], C.c_int),
+        "dl_partition": ([vp, vp, i64, i32, i32, vp, vp], C.c_int),
         "dl_build_hash_table": ([vp, vp, i64, C.c_double, pvp], C.c_int),
         "dl_hash_table_info": ([vp, pi64, pi64, pi64], C.c_int),
         "dl_hash_table_destroy": ([vp], C.c_int),

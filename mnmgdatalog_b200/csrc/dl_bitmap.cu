@@ -34,7 +34,9 @@ constexpr int TR_ROWS = 512;  // source rows per transpose tile
 constexpr int TR_WORDS = 16;  // source words (512 columns) per transpose tile
 constexpr int UT = 512;       // threads of the unit kernel
 
-// One source x and delta rows rows[start, start + len): paths x -> rows[i].
+// One source x and delta rows rows[start, start + len): paths x -> y for
+// the rows' targets y. A delta row holds the target's edge range (first edge,
+// out-degree) rather than the target itself: that is all a join needs.
 struct Unit {
     u32 x;
     u32 len;
@@ -67,6 +69,16 @@ __global__ void units_fill_kernel(const u32 *__restrict__ off, u64 n, u64 unit_r
     }
 }
 
+// Delta_0 rows: edge i (x -> y) as (off[y], deg y).
+__global__ void edge_rows_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, u64 ne,
+                                 uint2 *__restrict__ rows) {
+    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += (u64) gridDim.x * blockDim.x) {
+        const u32 y = val[i];
+        const u32 b = off[y];
+        rows[i] = make_uint2(b, off[y + 1] - b);
+    }
+}
+
 // sum over edges of the target's out-degree: the first join's size.
 __global__ void edge_degree_sum_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, u64 ne,
                                        unsigned long long *__restrict__ sum) {
@@ -79,27 +91,39 @@ __global__ void edge_degree_sum_kernel(const u32 *__restrict__ off, const u32 *_
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(sum, (unsigned long long) s);
 }
 
-constexpr int UW = UT / 32;   // warps of the unit kernel
-constexpr u32 SCHUNK = 8;     // summary words per warp chunk in the fold and emit phases
+constexpr int UW = UT / 32;      // warps of the unit kernel
+constexpr u32 SCHUNK = 8;        // summary words per warp chunk in the fold and emit phases
+constexpr u64 OCHUNK = 1 << 18;  // next-delta rows a CTA reserves at a time (a unit crossing the end of one is split)
+constexpr u64 UCHUNK = 16;       // next-delta unit slots a CTA reserves at a time
 
-struct UnitSmem {
+// Shared memory of the expansion of a unit's rows into a shared row.
+struct ExpandSmem {
     u32 wbeg[UW][32];   // per-warp compacted rows: first edge
     u32 wdeg[UW][32];   // and degree
+    u32 next_group;     // next row group to take
+};
+
+struct UnitSmem {
+    ExpandSmem e;
     u32 wrows[UW];      // per-warp new rows of the unit (fold phase)
-    u32 wbits[UW];      // per-warp new bits of the unit
-    u32 unit;
-    u32 next_group;
-    unsigned long long obase;
+    Unit cur;           // the unit being processed (len 0: none left)
+    Unit next;          // the next one, fetched while the current one runs
+    u64 ocur, oend;     // the CTA's reserved next-delta rows [ocur, oend)
+    u64 ucur, uend;     // and unit slots
+    u64 nbase;          // a fresh row reservation (when the unit does not fit the current one)
+    u64 pend_ocur, pend_oend;  // thread 0: the row reservation after the current unit
+    unsigned long long acc[UW][3];  // per warp: new tuples, next join size, rows written
     // followed by: u32 row[words], u32 summ[swords]
 };
 
 // Counters of one step (device, zeroed before the launch).
 struct StepCounters {
-    unsigned long long fetch;   // next unit to take
-    unsigned long long words;   // new tuples (next delta rows)
+    unsigned long long fetch;   // next unit slot to take
+    unsigned long long words;   // next-delta rows reserved (rows + unused tails of CTA reservations)
     unsigned long long join;    // join size of the next step
-    unsigned long long units;   // units of the next delta
+    unsigned long long units;   // next-delta unit slots reserved (unused ones hold len = 0)
     unsigned long long fresh;   // new tuples (|delta|; rows are written only for targets with out-edges)
+    unsigned long long rows;    // next-delta rows written
 };
 
 // hasout[k] bit b = node 32 k + b has out-edges (only those can join next step).
@@ -115,10 +139,88 @@ __global__ void hasout_kernel(const u32 *__restrict__ off, u64 n, u64 words, u32
 }
 
 // Next row group of the unit for this warp (lane 0 takes it, all lanes get it).
-__device__ __forceinline__ u32 take_group(UnitSmem &s, u32 lane) {
+__device__ __forceinline__ u32 take_group(ExpandSmem &s, u32 lane) {
     u32 g = 0;
     if (lane == 0) g = atomicAdd(&s.next_group, 1u);
     return __shfl_sync(0xffffffffu, g, 0);
+}
+
+// Join words of unit U into the shared row: for every delta row (an edge
+// range: first edge, degree), OR bit w into row[] for each edge target w, and
+// set summary bit w / 1024 when the word w / 32 goes from zero to non-zero.
+// Warps take groups of 32 rows; the next group's rows are loaded while the
+// current one is expanded, 32 join words at a time (the rows starting in a
+// window are a bit mask; a word's row is the number of rows started up to
+// its position), with the next window's edge-target load in flight before
+// the current window's shared-memory atomics. Called by every thread of the
+// CTA; s.next_group must be zero.
+__device__ __forceinline__ void expand_unit(ExpandSmem &s, u32 *row, u32 *summ, const uint2 *__restrict__ rows,
+                                            const u32 *__restrict__ val, const Unit &U, u32 lane, u32 warp, u32 lt,
+                                            u32 le) {
+    u32 grp = take_group(s, lane);
+    uint2 cur = make_uint2(0, 0);
+    if (grp * 32 + lane < U.len) cur = rows[U.start + grp * 32 + lane];
+    while (grp * 32 < U.len) {
+        const u32 grp1 = take_group(s, lane);
+        uint2 nxt = make_uint2(0, 0);
+        if (grp1 * 32 + lane < U.len) nxt = rows[U.start + grp1 * 32 + lane];
+        const u32 beg = cur.x, deg = cur.y;
+        const u32 nz = __ballot_sync(0xffffffffu, deg != 0);
+        if (nz) {
+            if (deg) {
+                const u32 rk = __popc(nz & lt);
+                s.wbeg[warp][rk] = beg;
+                s.wdeg[warp][rk] = deg;
+            }
+            __syncwarp();
+            const u32 nrows = __popc(nz);
+            const u32 cb = lane < nrows ? s.wbeg[warp][lane] : 0u;
+            const u32 cd = lane < nrows ? s.wdeg[warp][lane] : 0u;
+            __syncwarp();
+            const u32 incl = warp_inclusive_sum(cd);
+            const u32 pre = incl - cd;
+            const u32 total = __shfl_sync(0xffffffffu, incl, 31);
+            int base = -1;  // last row started before the window
+            // edge-target address of this lane's word of window i0
+            auto addr = [&](u32 i0) -> u32 {
+                const u32 st = (cd && pre >= i0 && pre < i0 + 32) ? 1u << (pre - i0) : 0u;
+                const u32 starts = __reduce_or_sync(0xffffffffu, st);
+                const int o = base + __popc(starts & le);
+                base += __popc(starts);
+                const u32 ob = __shfl_sync(0xffffffffu, cb, o);
+                const u32 op = __shfl_sync(0xffffffffu, pre, o);
+                return ob + (i0 + lane - op);
+            };
+            const u32 a0 = addr(0);  // warp-collective: every lane calls it
+            u32 w = lane < total ? __ldg(val + a0) : 0u;
+            for (u32 i0 = 0; i0 < total; i0 += 32) {
+                const bool have = i0 + lane < total;
+                u32 wn = 0;
+                if (i0 + 32 < total) {
+                    const u32 a = addr(i0 + 32);
+                    if (i0 + 32 + lane < total) wn = __ldg(val + a);
+                }
+                if (have) {
+                    const u32 old = atomicOr(&row[w >> 5], 1u << (w & 31));
+                    if (old == 0) atomicOr(&summ[w >> 10], 1u << ((w >> 5) & 31));
+                }
+                w = wn;
+            }
+        }
+        grp = grp1;
+        cur = nxt;
+    }
+}
+
+// The next non-empty unit from the shared queue (len 0: none left). Called by
+// one thread.
+__device__ __forceinline__ Unit fetch_unit(const Unit *__restrict__ units, u64 nunits, StepCounters *ctr) {
+    for (;;) {
+        const u64 i = atomicAdd(&ctr->fetch, 1ull);
+        if (i >= nunits) return Unit{0, 0, 0};
+        const Unit u = units[i];
+        if (u.len) return u;
+    }
 }
 
 // One semi-naive TC step over the units of a delta (persistent CTAs).
@@ -129,13 +231,19 @@ __device__ __forceinline__ u32 take_group(UnitSmem &s, u32 lane) {
 // touches a word). The fold then visits only touched words: one atomicOr
 // (with return) on the matrix per word, coalesced over 32 consecutive words;
 // new bits = row & ~old, and those whose target has out-edges become rows of
-// the next delta. The emit visits only words with such rows and writes them
-// warp-cooperatively (one ballot per non-zero word, consecutive positions).
-// Phases are separated by four CTA barriers per unit.
+// the next delta, which the emit writes from the words that hold them.
+//
+// Latency is hidden rather than waited for: the next unit is fetched while
+// the current one runs; each warp loads the next row group's rows and edge
+// offsets while it expands the current group; next-delta rows and unit slots
+// come from per-CTA reservations (a global atomic only when one runs out);
+// counters are summed per thread and added once at the end. Three CTA
+// barriers separate a unit's phases (a fourth only when a row reservation
+// runs out).
 __global__ void __launch_bounds__(UT, 4)
-bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const u32 *__restrict__ rows,
+bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const uint2 *__restrict__ rows,
                         const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
-                        u32 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap, u64 unit_rows,
+                        uint2 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap, u64 unit_rows,
                         const u32 *__restrict__ hasout, StepCounters *__restrict__ ctr, u32 *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     UnitSmem &s = *reinterpret_cast<UnitSmem *>(smem_raw);
@@ -147,81 +255,32 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
     const u32 le = lane == 31 ? ~0u : (2u << lane) - 1;  // lanes <= lane
     const u32 nchunks = (swords + SCHUNK - 1) / SCHUNK;
     for (u32 k = tid; k < words + swords; k += UT) row[k] = 0;
-    if (tid == 0) s.next_group = 0;
+    if (tid == 0) {
+        s.e.next_group = 0;
+        s.ocur = s.oend = s.ucur = s.uend = s.pend_ocur = s.pend_oend = 0;
+        s.next = fetch_unit(units, nunits, ctr);
+    }
+    if (lane == 0) s.acc[warp][0] = s.acc[warp][1] = s.acc[warp][2] = 0;
     for (;;) {
-        if (tid == 0) s.unit = (u32) min((unsigned long long) nunits, atomicAdd(&ctr->fetch, 1ull));
-        __syncthreads();  // (1) unit taken; row, summary and group counter are clear
-        const u64 ui = s.unit;
-        if (ui >= nunits) break;
-        const Unit U = units[ui];
-        // ---- join words (x, w) of the unit into the shared row ----
-        // Warps take groups of 32 rows; the next group's rows are loaded while
-        // the current one is expanded, 32 join words at a time (the rows
-        // starting in a window are a bit mask; a word's row is the number of
-        // rows started up to its position), with the next window's edge-target
-        // load in flight before the current window's shared-memory atomics.
-        u32 grp = take_group(s, lane);
-        u32 ny = 0;
-        if (grp * 32 + lane < U.len) ny = rows[U.start + grp * 32 + lane];
-        while (grp * 32 < U.len) {
-            const u32 r = grp * 32 + lane;
-            u32 beg = 0, deg = 0;
-            if (r < U.len) {
-                beg = __ldg(off + ny);
-                deg = __ldg(off + ny + 1) - beg;
-            }
-            const u32 ngrp = take_group(s, lane);
-            if (ngrp * 32 + lane < U.len) ny = rows[U.start + ngrp * 32 + lane];
-            const u32 nz = __ballot_sync(0xffffffffu, deg != 0);
-            if (nz) {
-                if (deg) {
-                    const u32 rk = __popc(nz & lt);
-                    s.wbeg[warp][rk] = beg;
-                    s.wdeg[warp][rk] = deg;
-                }
-                __syncwarp();
-                const u32 nrows = __popc(nz);
-                beg = lane < nrows ? s.wbeg[warp][lane] : 0u;
-                deg = lane < nrows ? s.wdeg[warp][lane] : 0u;
-                __syncwarp();
-                const u32 incl = warp_inclusive_sum(deg);
-                const u32 pre = incl - deg;
-                const u32 total = __shfl_sync(0xffffffffu, incl, 31);
-                int base = -1;  // last row started before the window
-                // edge-target address of this lane's word of window i0
-                auto addr = [&](u32 i0) -> u32 {
-                    const u32 st = (deg && pre >= i0 && pre < i0 + 32) ? 1u << (pre - i0) : 0u;
-                    const u32 starts = __reduce_or_sync(0xffffffffu, st);
-                    const int o = base + __popc(starts & le);
-                    base += __popc(starts);
-                    const u32 ob = __shfl_sync(0xffffffffu, beg, o);
-                    const u32 op = __shfl_sync(0xffffffffu, pre, o);
-                    return ob + (i0 + lane - op);
-                };
-                const u32 a0 = addr(0);  // warp-collective: every lane calls it
-                u32 w = lane < total ? __ldg(val + a0) : 0u;
-                for (u32 i0 = 0; i0 < total; i0 += 32) {
-                    const bool have = i0 + lane < total;
-                    u32 wn = 0;
-                    if (i0 + 32 < total) {
-                        const u32 a = addr(i0 + 32);
-                        if (i0 + 32 + lane < total) wn = __ldg(val + a);
-                    }
-                    if (have) {
-                        const u32 old = atomicOr(&row[w >> 5], 1u << (w & 31));
-                        if (old == 0) atomicOr(&summ[w >> 10], 1u << ((w >> 5) & 31));
-                    }
-                    w = wn;
-                }
-            }
-            grp = ngrp;
+        if (tid == 0) s.cur = s.next;
+        __syncthreads();  // (1) unit known; row, summary and group counter are clear
+        const Unit U = s.cur;
+        if (U.len == 0) break;
+        if (tid == 0) {
+            // every thread read the previous unit's reservation before this
+            // barrier; the new one is read after barrier (3)
+            s.ocur = s.pend_ocur;
+            s.oend = s.pend_oend;
+            s.next = fetch_unit(units, nunits, ctr);  // read only at the next barrier (1)
         }
+        // ---- join words (x, w) of the unit into the shared row ----
+        expand_unit(s.e, row, summ, rows, val, U, lane, warp, lt, le);
         __syncthreads();  // (2) the row is complete
         // ---- fold the touched words into M: new bits = row & ~M ----
         // Every new bit counts in |delta|; only targets with out-edges become
         // rows of the next delta. Warp w takes summary chunks w, w + UW, ...
         const u64 mrow = (u64) U.x * stride;
-        u32 nrows_w = 0, nbits_w = 0;
+        u32 nrows_w = 0, fresh = 0;
         for (u32 c = warp; c < nchunks; c += UW) {
             const u32 sw0 = c * SCHUNK;
             const u32 sv = (lane < SCHUNK && sw0 + lane < swords) ? summ[sw0 + lane] : 0u;
@@ -237,14 +296,14 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                 const bool a0 = (s0 >> lane) & 1, a1 = j1 < 32 && ((s1 >> lane) & 1);
                 const u32 k0 = (sw0 + j0) * 32 + lane, k1 = (sw0 + (j1 & 31)) * 32 + lane;
                 const u32 v0 = a0 ? row[k0] : 0u, v1 = a1 ? row[k1] : 0u;
+                const u32 h0 = a0 ? __ldg(hasout + k0) : 0u, h1 = a1 ? __ldg(hasout + k1) : 0u;
                 const u32 o0 = a0 ? atomicOr(&m[mrow + k0], v0) : ~0u;
                 const u32 o1 = a1 ? atomicOr(&m[mrow + k1], v1) : ~0u;
-                const u32 h0 = a0 ? __ldg(hasout + k0) : 0u, h1 = a1 ? __ldg(hasout + k1) : 0u;
                 const u32 f0 = v0 & ~o0, f1 = v1 & ~o1;
                 const u32 r0 = f0 & h0, r1 = f1 & h1;
                 if (a0) row[k0] = r0;
                 if (a1) row[k1] = r1;
-                nbits_w += __popc(f0) + __popc(f1);
+                fresh += __popc(f0) + __popc(f1);
                 nrows_w += __popc(r0) + __popc(r1);
                 const u32 m0 = __ballot_sync(0xffffffffu, r0 != 0);
                 const u32 m1 = __ballot_sync(0xffffffffu, r1 != 0);
@@ -255,28 +314,43 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
             }
         }
         nrows_w = warp_sum(nrows_w);
-        nbits_w = warp_sum(nbits_w);
-        if (lane == 0) {
-            s.wrows[warp] = nrows_w;
-            s.wbits[warp] = nbits_w;
-        }
+        if (lane == 0) s.wrows[warp] = nrows_w;
         __syncthreads();  // (3) per-warp counts
         const u32 cw = lane < UW ? s.wrows[lane] : 0u;
-        const u32 bw = lane < UW ? s.wbits[lane] : 0u;
         const u32 cinc = warp_inclusive_sum(cw);
         const u32 total = __shfl_sync(0xffffffffu, cinc, 31);
         const u32 before = __shfl_sync(0xffffffffu, cinc - cw, warp);  // new rows of lower warps
-        const u32 fresh = warp_sum(bw);
-        if (tid == 0) {
-            s.obase = total ? atomicAdd(&ctr->words, (unsigned long long) total) : 0ull;
-            if (fresh) atomicAdd(&ctr->fresh, (unsigned long long) fresh);
+        // The unit's rows go to the CTA's reservation [ocur, oend); what does
+        // not fit goes to a fresh one [nb, ...) (every thread reads the same
+        // words, so all take the same branch). Unit-relative position i lands
+        // at ocur + i below `avail`, at nb + (i - avail) above.
+        const u64 ocur = s.ocur;
+        const u64 avail = min((u64) total, s.oend - ocur);
+        u64 nb = 0;
+        if (total > avail) {
+            if (tid == 0) {
+                const u64 need = total - avail;
+                const u64 size = max(need, OCHUNK);
+                s.nbase = atomicAdd(&ctr->words, (unsigned long long) size);
+                s.pend_ocur = s.nbase + need;
+                s.pend_oend = s.nbase + size;
+            }
+            __syncthreads();  // (4, when a reservation runs out) the fresh one
+            nb = s.nbase;
+        } else if (tid == 0) {
+            s.pend_ocur = ocur + total;  // s.ocur takes it after the next barrier (1)
+            s.pend_oend = s.oend;
         }
-        __syncthreads();  // (4) the unit's place in the next delta
-        const u64 obase = s.obase;
         // ---- emit the new rows (targets of x) and clear the row ----
         // New bits are sparse within a word, so each lane walks its own word.
-        u64 p = obase + before;
-        u64 dsum = 0;
+        // A row is written as the target's edge range; its loads are in flight
+        // while the lane moves on to the next bit (the row is stored one bit
+        // later), and its degree adds to the next join size.
+        u64 p = before;  // unit-relative position
+        u32 dsum = 0;
+        bool pend = false;
+        uint2 prow = make_uint2(0, 0);
+        u64 pq = 0;
         for (u32 c = warp; c < nchunks; c += UW) {
             const u32 sw0 = c * SCHUNK;
             const u32 sv = (lane < SCHUNK && sw0 + lane < swords) ? summ[sw0 + lane] : 0u;
@@ -295,34 +369,298 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
                 const u32 cnt = __popc(fr);
                 const u32 incl = warp_inclusive_sum(cnt);
                 u64 q = p + (incl - cnt);
+                const u32 tb = (kb + lane) * 32;
                 while (fr) {
-                    const u32 t = (kb + lane) * 32 + (__ffs(fr) - 1);
+                    const u32 t = tb + (__ffs(fr) - 1);
                     fr &= fr - 1;
-                    if (q < out_cap) out[q] = t;
-                    else atomicOr(err, DL_DEVERR_CAPACITY);  // more new tuples than join words: reported
-                    ++q;
-                    dsum += __ldg(off + t + 1) - __ldg(off + t);
+                    const u32 b = __ldg(off + t), e = __ldg(off + t + 1);
+                    if (pend) {
+                        const u64 a = pq < avail ? ocur + pq : nb + (pq - avail);
+                        if (a < out_cap) out[a] = make_uint2(prow.x, prow.y - prow.x);
+                        else atomicOr(err, DL_DEVERR_CAPACITY);  // more rows than reserved: reported
+                        dsum += prow.y - prow.x;
+                    }
+                    prow = make_uint2(b, e);
+                    pq = q++;
+                    pend = true;
                 }
                 p += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
-        // rows of the row words untouched by the fold are already zero; the
-        // touched ones were zeroed in the fold (no new rows) or just now
-        dsum = warp_sum(dsum);
-        if (lane == 0 && dsum) atomicAdd(&ctr->join, (unsigned long long) dsum);
-        if (warp == 0 && total) {
-            const u64 nsub = (total + unit_rows - 1) / unit_rows;
-            u64 ub = 0;
-            if (lane == 0) ub = atomicAdd(&ctr->units, (unsigned long long) nsub);
-            ub = __shfl_sync(0xffffffffu, ub, 0);
-            for (u64 i = lane; i < nsub; i += 32) {
-                if (ub + i < uout_cap)
-                    uout[ub + i] = Unit{U.x, (u32) min(unit_rows, total - i * unit_rows), obase + i * unit_rows};
-                else
-                    atomicOr(err, DL_DEVERR_CAPACITY);
+        if (pend) {
+            const u64 a = pq < avail ? ocur + pq : nb + (pq - avail);
+            if (a < out_cap) out[a] = make_uint2(prow.x, prow.y - prow.x);
+            else atomicOr(err, DL_DEVERR_CAPACITY);
+            dsum += prow.y - prow.x;
+        }
+        {
+            const u32 fw = warp_sum(fresh);
+            const u64 dw = warp_sum((u64) dsum);
+            if (lane == 0) {
+                s.acc[warp][0] += fw;
+                s.acc[warp][1] += dw;
+                s.acc[warp][2] += nrows_w;
             }
         }
-        if (tid == 0) s.next_group = 0;  // read again only after barrier (1)
+        // The unit's entries of the next delta (at most unit_rows rows each,
+        // one range per reservation): slots from the CTA's reservation of unit
+        // slots (thread 0 only).
+        if (tid == 0 && total) {
+            for (int part = 0; part < 2; ++part) {
+                const u64 len = part == 0 ? avail : total - avail;
+                const u64 start = part == 0 ? ocur : nb;
+                for (u64 i = 0; i < len; i += unit_rows) {
+                    if (s.ucur == s.uend) {
+                        s.ucur = atomicAdd(&ctr->units, (unsigned long long) UCHUNK);
+                        s.uend = s.ucur + UCHUNK;
+                    }
+                    const u64 slot = s.ucur++;
+                    if (slot < uout_cap)
+                        uout[slot] = Unit{U.x, (u32) min(unit_rows, len - i), start + i};
+                    else
+                        atomicOr(err, DL_DEVERR_CAPACITY);
+                }
+            }
+        }
+        if (tid == 0) s.e.next_group = 0;  // read again only after barrier (1)
+    }
+    // Unused reserved unit slots become empty units (skipped by fetch_unit).
+    if (tid == 0)
+        for (u64 slot = s.ucur; slot < s.uend; ++slot)
+            if (slot < uout_cap) uout[slot] = Unit{0, 0, 0};
+    if (lane == 0) {
+        if (s.acc[warp][0]) atomicAdd(&ctr->fresh, s.acc[warp][0]);
+        if (s.acc[warp][1]) atomicAdd(&ctr->join, s.acc[warp][1]);
+        if (s.acc[warp][2]) atomicAdd(&ctr->rows, s.acc[warp][2]);
+    }
+}
+
+// ---- SG on the bit matrix ----------------------------------------------
+//
+// sg(x, y) :- e(a, x), sg(a, b), e(b, y): with full as a bit matrix M (row x,
+// column y), the new tuples of a delta unit (a, rows b) are
+// R & ~M[x] for every x in e(a, .), where R = the union of e(b, .) over the
+// unit's rows -- the same shared-memory row the TC step builds, folded into
+// every row x of a's out-edges instead of into row a. The base rule
+// sg(x, y) :- e(p, x), e(p, y), x != y is the same step on the units
+// (p, rows {p}) with bit x cleared from R when it is folded into row x.
+struct SgSmem {
+    ExpandSmem e;
+    Unit cur, next;
+    u32 next_x;                      // next fold target of the unit (a's out-edge index)
+    u32 nlist;                       // touched words of R in the list
+    u64 res[UW][4];                  // per warp: next-delta rows [cur, end), unit slots [cur, end)
+    unsigned long long acc[UW][3];   // per warp: new tuples, next-step bound, rows written
+    // followed by: u32 row[words], u32 summ[swords], u32 lk[words], u32 lv[words]
+    // (the touched words of R as a list: index, value)
+};
+
+constexpr u64 WCHUNK = 4096;  // next-delta rows a warp reserves at a time
+
+// Writes the units of one fold target x: rows [start, start + len) of the
+// next delta (at most unit_rows per unit), slots from the warp's reservation.
+// Lane 0 only.
+__device__ __forceinline__ void sg_close_range(u64 *res, u32 x, u64 start, u64 len, u64 unit_rows,
+                                               Unit *__restrict__ uout, u64 uout_cap, StepCounters *ctr, u32 *err) {
+    for (u64 i = 0; i < len; i += unit_rows) {
+        if (res[2] == res[3]) {
+            res[2] = atomicAdd(&ctr->units, (unsigned long long) UCHUNK);
+            res[3] = res[2] + UCHUNK;
+        }
+        const u64 slot = res[2]++;
+        if (slot < uout_cap) uout[slot] = Unit{x, (u32) min(unit_rows, len - i), start + i};
+        else atomicOr(err, DL_DEVERR_CAPACITY);
+    }
+}
+
+__global__ void __launch_bounds__(UT, 4)
+sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const uint2 *__restrict__ rows,
+                    const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
+                    uint2 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap, u64 unit_rows,
+                    const u32 *__restrict__ hasout, StepCounters *__restrict__ ctr, u32 *err, int base_rule) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SgSmem &s = *reinterpret_cast<SgSmem *>(smem_raw);
+    u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(SgSmem));
+    const u32 swords = (words + 31) / 32;
+    u32 *summ = row + words;
+    u32 *lk = summ + swords;
+    u32 *lv = lk + words;
+    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const u32 lt = lanemask_lt();
+    const u32 le = lane == 31 ? ~0u : (2u << lane) - 1;
+    const u32 nchunks = (swords + SCHUNK - 1) / SCHUNK;
+    for (u32 k = tid; k < words + swords; k += UT) row[k] = 0;
+    if (lane == 0) {
+        s.res[warp][0] = s.res[warp][1] = s.res[warp][2] = s.res[warp][3] = 0;
+        s.acc[warp][0] = s.acc[warp][1] = s.acc[warp][2] = 0;
+    }
+    if (tid == 0) {
+        s.e.next_group = 0;
+        s.nlist = 0;
+        s.next = fetch_unit(units, nunits, ctr);
+    }
+    for (;;) {
+        if (tid == 0) {
+            s.cur = s.next;
+            s.next_x = 0;
+        }
+        __syncthreads();  // (1) unit known; row, summary, group and target counters are clear
+        const Unit U = s.cur;
+        if (U.len == 0) break;
+        if (tid == 0) s.next = fetch_unit(units, nunits, ctr);  // read only at the next barrier (1)
+        expand_unit(s.e, row, summ, rows, val, U, lane, warp, lt, le);
+        __syncthreads();  // (2) R is complete
+        // ---- the touched words of R as a list (index, value), any order ----
+        for (u32 sw = tid; sw < swords; sw += UT) {
+            u32 bits = summ[sw];
+            if (!bits) continue;
+            u32 at = atomicAdd(&s.nlist, (u32) __popc(bits));
+            while (bits) {
+                const u32 k = sw * 32 + (__ffs(bits) - 1);
+                bits &= bits - 1;
+                lk[at] = k;
+                lv[at] = row[k];
+                ++at;
+            }
+        }
+        __syncthreads();  // (3) the list is complete
+        const u32 nlist = s.nlist;
+        // ---- fold R into every row x of a's out-edges; emit each x's new rows ----
+        // A warp takes one x at a time and walks the list 32 words per step,
+        // the 32 matrix atomics of a step in flight together. A new row is
+        // written as its target's edge range, one bit later than its loads.
+        const u32 xb = __ldg(off + U.x), xn = __ldg(off + U.x + 1) - xb;
+        u32 fresh = 0, rows_w = 0;
+        u64 bound = 0;  // sum over new rows (x, y) of deg(x) deg(y): the next step's new tuples are below it
+        for (;;) {
+            u32 i = 0;
+            if (lane == 0) i = atomicAdd(&s.next_x, 1u);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= xn) break;
+            const u32 x = __ldg(val + xb + i);
+            const u32 ox = __ldg(off + x);
+            const u32 dx = __ldg(off + x + 1) - ox;  // fold fan-out of a unit of x next step
+            const u64 mrow = (u64) x * stride;
+            const u32 self_word = base_rule ? (x >> 5) : ~0u;
+            u64 *res = s.res[warp];
+            u64 xstart = res[0], cur = res[0];
+            bool pend = false;
+            u64 pa = 0;
+            uint2 prow = make_uint2(0, 0);
+            for (u32 c0 = 0; c0 < nlist; c0 += 32) {
+                const bool have = c0 + lane < nlist;
+                const u32 k = have ? lk[c0 + lane] : 0u;
+                u32 v = have ? lv[c0 + lane] : 0u;
+                if (k == self_word) v &= ~(1u << (x & 31));  // base rule: x != y
+                const u32 o = v ? atomicOr(&m[mrow + k], v) : ~0u;
+                const u32 f = v & ~o;
+                fresh += __popc(f);
+                const u32 fr = (f && dx) ? f & __ldg(hasout + k) : 0u;  // rows only if both can join
+                const u32 cnt = __popc(fr);
+                const u32 incl = warp_inclusive_sum(cnt);
+                const u32 tot = __shfl_sync(0xffffffffu, incl, 31);
+                if (!tot) continue;
+                if (cur + tot > res[1]) {  // the warp's reservation runs out: close x's range so far
+                    if (pend) {  // the pending row belongs to the range being closed
+                        if (pa < out_cap) out[pa] = make_uint2(prow.x, prow.y - prow.x);
+                        else atomicOr(err, DL_DEVERR_CAPACITY);
+                        bound += (u64) (prow.y - prow.x) * dx;
+                        pend = false;
+                    }
+                    if (lane == 0) {
+                        sg_close_range(res, x, xstart, cur - xstart, unit_rows, uout, uout_cap, ctr, err);
+                        const u64 size = max((u64) tot, WCHUNK);
+                        res[0] = atomicAdd(&ctr->words, (unsigned long long) size);
+                        res[1] = res[0] + size;
+                    }
+                    __syncwarp();
+                    xstart = cur = res[0];
+                }
+                u64 q = cur + (incl - cnt);
+                u32 bits = fr;
+                while (bits) {
+                    const u32 t = k * 32 + (__ffs(bits) - 1);
+                    bits &= bits - 1;
+                    const u32 b = __ldg(off + t), e = __ldg(off + t + 1);
+                    if (pend) {
+                        if (pa < out_cap) out[pa] = make_uint2(prow.x, prow.y - prow.x);
+                        else atomicOr(err, DL_DEVERR_CAPACITY);  // reported: the host reruns on the sorted runs
+                        bound += (u64) (prow.y - prow.x) * dx;
+                    }
+                    prow = make_uint2(b, e);
+                    pa = q++;
+                    pend = true;
+                }
+                cur += tot;
+                rows_w += cnt;
+            }
+            if (pend) {
+                if (pa < out_cap) out[pa] = make_uint2(prow.x, prow.y - prow.x);
+                else atomicOr(err, DL_DEVERR_CAPACITY);
+                bound += (u64) (prow.y - prow.x) * dx;
+            }
+            if (lane == 0) {
+                sg_close_range(res, x, xstart, cur - xstart, unit_rows, uout, uout_cap, ctr, err);
+                res[0] = cur;
+            }
+            __syncwarp();
+        }
+        {
+            const u32 fw = warp_sum(fresh), rw = warp_sum(rows_w);
+            const u64 bw = warp_sum(bound);
+            if (lane == 0) {
+                s.acc[warp][0] += fw;
+                s.acc[warp][1] += bw;
+                s.acc[warp][2] += rw;
+            }
+        }
+        __syncthreads();  // (4) every fold target is done with R
+        // ---- clear R and its summary (the list holds every touched word) ----
+        for (u32 i2 = tid; i2 < nlist; i2 += UT) {
+            const u32 k = lk[i2];
+            row[k] = 0;
+            summ[k >> 5] = 0;
+        }
+        if (tid == 0) s.nlist = 0;  // read again only after barrier (3)
+        if (tid == 0) s.e.next_group = 0;  // read again only after barrier (1)
+    }
+    // Unused reserved unit slots become empty units (skipped by fetch_unit).
+    if (lane == 0) {
+        for (u64 slot = s.res[warp][2]; slot < s.res[warp][3]; ++slot)
+            if (slot < uout_cap) uout[slot] = Unit{0, 0, 0};
+        if (s.acc[warp][0]) atomicAdd(&ctr->fresh, s.acc[warp][0]);
+        if (s.acc[warp][1]) atomicAdd(&ctr->join, s.acc[warp][1]);
+        if (s.acc[warp][2]) atomicAdd(&ctr->rows, s.acc[warp][2]);
+    }
+}
+
+// Base units of SG: node p -> row p = (off[p], deg p) and unit (p, rows {p})
+// (empty when p has no out-edges); *bound += deg(p)^2, the base's new tuples
+// are below it.
+__global__ void sg_base_units_kernel(const u32 *__restrict__ off, u64 n, uint2 *__restrict__ rows,
+                                     Unit *__restrict__ units, unsigned long long *__restrict__ bound) {
+    u64 b2 = 0;
+    for (u64 p = (u64) blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (u64) gridDim.x * blockDim.x) {
+        const u32 b = off[p], d = off[p + 1] - b;
+        rows[p] = make_uint2(b, d);
+        units[p] = Unit{(u32) p, d ? 1u : 0u, p};
+        b2 += (u64) d * d;
+    }
+    b2 = warp_sum(b2);
+    if ((threadIdx.x & 31) == 0 && b2) atomicAdd(bound, (unsigned long long) b2);
+}
+
+// Row sums: counts[x] = set bits of row x among its first `words` words.
+__global__ void bitmat_row_popc_kernel(const u32 *__restrict__ m, u64 n, u64 stride, u64 words,
+                                       unsigned long long *__restrict__ counts) {
+    const u32 lane = threadIdx.x & 31;
+    const u64 warps = (u64) gridDim.x * (blockDim.x / 32);
+    for (u64 x = ((u64) blockIdx.x * blockDim.x + threadIdx.x) / 32; x < n; x += warps) {
+        const u32 *r = m + x * stride;
+        u32 c = 0;
+        for (u64 k = lane; k < words; k += 32) c += __popc(__ldcs(r + k));
+        c = warp_sum(c);
+        if (lane == 0) counts[x] = c;
     }
 }
 
@@ -373,14 +711,23 @@ __global__ void __launch_bounds__(TR_ROWS, 2) bitmat_transpose_count_kernel(cons
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const u64 c0 = (u64) blockIdx.x * TR_WORDS;  // first column word of the block
     const u64 nblocks = (n + TR_ROWS - 1) / TR_ROWS;
+    // A column block lies inside the row (stride is a multiple of 32 words);
+    // only the last block of source rows and of target rows can be partial.
+    const bool full_targets = c0 * 32 + TR_ROWS <= n;
+    const u32 r0 = tid / TR_WORDS, cc = tid % TR_WORDS;  // this thread's first (row, word) of a tile
     auto issue = [&](u64 b, int buf) {  // tile (b, c) -> in[buf]
         const u64 x0 = b * TR_ROWS;
+        const u32 *src = a + (x0 + r0) * stride + c0 + cc;
+        const u64 step = (u64) (TR_ROWS / TR_WORDS) * stride;  // 32 rows
+        if (x0 + TR_ROWS <= n) {
 #pragma unroll
-        for (u32 j = 0; j < TR_WORDS; ++j) {
-            const u32 i = tid + j * TR_ROWS, r = i / TR_WORDS, c = i % TR_WORDS;
-            const u64 x = x0 + r, col = c0 + c;
-            if (x < n && col < stride) cp_async4(&in[buf][r][c], a + x * stride + col);
-            else in[buf][r][c] = 0u;
+            for (u32 j = 0; j < TR_WORDS; ++j) cp_async4(&in[buf][r0 + 32 * j][cc], src + j * step);
+        } else {
+#pragma unroll
+            for (u32 j = 0; j < TR_WORDS; ++j) {
+                if (x0 + r0 + 32 * j < n) cp_async4(&in[buf][r0 + 32 * j][cc], src + j * step);
+                else in[buf][r0 + 32 * j][cc] = 0u;
+            }
         }
     };
     u32 cnt = 0;  // set bits of target row c0 * 32 + tid in this CTA's tiles
@@ -402,12 +749,15 @@ __global__ void __launch_bounds__(TR_ROWS, 2) bitmat_transpose_count_kernel(cons
 #pragma unroll
         for (u32 xw = 0; xw < TR_ROWS / 32; ++xw) cnt += __popc(outw[tid][xw]);
         const u64 x0 = b * TR_ROWS;
+        u32 *dst = t + (c0 * 32 + r0) * stride + x0 / 32 + cc;
+        const u64 step = (u64) (TR_ROWS / TR_WORDS) * stride;  // 32 target rows
+        if (full_targets) {
 #pragma unroll 4
-        for (u32 j = 0; j < TR_WORDS; ++j) {
-            const u32 i = tid + j * TR_ROWS;
-            const u32 r = i / (TR_ROWS / 32), xw = i % (TR_ROWS / 32);
-            const u64 w = c0 * 32 + r, col = x0 / 32 + xw;
-            if (w < n && col < stride) t[w * stride + col] = outw[r][xw];
+            for (u32 j = 0; j < TR_WORDS; ++j) dst[j * step] = outw[r0 + 32 * j][cc];
+        } else {
+#pragma unroll 4
+            for (u32 j = 0; j < TR_WORDS; ++j)
+                if (c0 * 32 + r0 + 32 * j < n) dst[j * step] = outw[r0 + 32 * j][cc];
         }
         // outw is rewritten only after the next iteration's first barrier
     }
@@ -415,19 +765,31 @@ __global__ void __launch_bounds__(TR_ROWS, 2) bitmat_transpose_count_kernel(cons
     if (w < n && cnt) atomicAdd(counts + w, (unsigned long long) cnt);
 }
 
-// Row w of t -> result rows (ids[x], ids[w]) for its set bits x, ascending,
-// from out[first[w]] on: the reference's TC file order (x, z) sorted by
-// (z, x). One warp per row; a lane takes 4 consecutive words per step (one
+// Row w of t -> result rows for its set bits x, ascending, from
+// out[first[w]] on: (ids[x], ids[w]) for TC's transpose (the reference's TC
+// file order (x, z) sorted by (z, x)), (ids[w], ids[x]) for SG's matrix (its
+// order (x, y) sorted by (x, y)). One warp per row; a lane takes 4 consecutive words per step (one
 // 16-byte load, the next one in flight); a step's rows are staged in shared
 // memory and leave with consecutive stores unless there are more than
 // EX_STAGE of them. (Result words are sparse -- C1 averages well under one
 // set bit per non-zero word -- so each lane walks its own words' bits.)
 constexpr int EX_THREADS = 256;
 constexpr int EX_STAGE = 256;
+// a result row as one little-endian 8-byte word: (column id, row id) for TC
+// (rows (x, z) of the transpose's row z), (row id, column id) for SG
+template <bool RowFirst>
+__device__ __forceinline__ u64 pack_row(u32 row_id, u32 col_id) {
+    return RowFirst ? ((u64) col_id << 32) | row_id : ((u64) row_id << 32) | col_id;
+}
+__device__ __forceinline__ u32 xid(const int32_t *__restrict__ ids, bool affine, int32_t base, u64 x) {
+    return (u32) (affine ? (int32_t) (base + (int64_t) x) : __ldg(ids + x));
+}
+template <bool RowFirst>
 __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u32 *__restrict__ t, u64 n,
                                                                          u64 stride, u64 words,
                                                                          const u64 *__restrict__ first,
                                                                          const int32_t *__restrict__ ids,
+                                                                         bool affine, int32_t base,
                                                                          u64 *__restrict__ out) {
     __shared__ u64 stage[EX_THREADS / 32][EX_STAGE];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -436,15 +798,19 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u
     for (u64 w = (u64) blockIdx.x * (EX_THREADS / 32) + warp; w < n; w += warps) {
         const u32 *row = t + w * stride;
         u64 pos = first[w];
-        const u64 hi = (u64) (u32) ids[w] << 32;  // (x id, z id) as one little-endian 8-byte row
-        // stride is a multiple of 32 words: a lane's vector stays in the row
-        uint4 nxt = make_uint4(0, 0, 0, 0);
-        if ((u64) lane * 4 < words) nxt = __ldcs(reinterpret_cast<const uint4 *>(row + lane * 4));
+        // a dense id range needs no table lookup (ids[r] == base + r)
+        const u32 idw = (u32) (affine ? (int32_t) (base + (int64_t) w) : ids[w]);
+        // stride is a multiple of 32 words: a lane's vector stays in the row.
+        // Two steps' loads are in flight while a step is emitted.
+        auto load = [&](u64 k) {
+            return k < words ? __ldcs(reinterpret_cast<const uint4 *>(row + k)) : make_uint4(0, 0, 0, 0);
+        };
+        uint4 n1 = load((u64) lane * 4), n2 = load((u64) lane * 4 + 128);
         for (u64 k0 = 0; k0 < words; k0 += 128) {
             const u64 k = k0 + lane * 4;
-            const uint4 q = nxt;  // this step's words; the next step's load is in flight meanwhile
-            nxt = make_uint4(0, 0, 0, 0);
-            if (k + 128 < words) nxt = __ldcs(reinterpret_cast<const uint4 *>(row + k + 128));
+            const uint4 q = n1;
+            n1 = n2;
+            n2 = load(k + 256);
             u32 v[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
             for (int c = 0; c < 4; ++c)
@@ -458,7 +824,7 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
                     for (u32 b = v[c]; b; b &= b - 1)
-                        st[p++] = hi | (u32) __ldg(ids + (k + c) * 32 + (__ffs(b) - 1));
+                        st[p++] = pack_row<RowFirst>(idw, xid(ids, affine, base, (k + c) * 32 + (__ffs(b) - 1)));
                 __syncwarp();
                 for (u32 i = lane; i < sum; i += 32) out[pos + i] = st[i];
                 __syncwarp();
@@ -467,7 +833,7 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
                     for (u32 b = v[c]; b; b &= b - 1)
-                        out[q2++] = hi | (u32) __ldg(ids + (k + c) * 32 + (__ffs(b) - 1));
+                        out[q2++] = pack_row<RowFirst>(idw, xid(ids, affine, base, (k + c) * 32 + (__ffs(b) - 1)));
             }
             pos += sum;
         }
@@ -500,9 +866,11 @@ u64 exclusive_scan(Context &ctx, const u64 *in, u64 n, u64 *out) {
 u64 bitmat_stride(u64 n) { return ((n + 31) / 32 + 31) / 32 * 32; }
 u64 bitmat_bytes(u64 n) { return n * bitmat_stride(n) * 4; }
 
-bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n) {
+bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, int copies) {
     if (opt.dedup != DL_DEDUP_AUTO && opt.dedup != DL_DEDUP_BITMAP) return false;
-    const u64 need = 2 * bitmat_bytes(n);
+    // a row (TC), or a row and its touched-word list (SG), must fit in shared memory
+    if ((n + 31) / 32 * 4 * (copies == 1 ? 3 : 1) + sizeof(SgSmem) + 4096 > 227 * 1024) return false;
+    const u64 need = (u64) copies * bitmat_bytes(n);
     size_t free_b = 0, total_b = 0;
     DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const u64 held = ctx.ws.bitmat[0].cap + ctx.ws.bitmat[1].cap;
@@ -533,8 +901,9 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
     DL_CUDA(cudaMemsetAsync(M.p, 0, bitmat_bytes(n), ctx.stream));
     u32 *m = M.as<u32>();
     StepCounters *ctr = reinterpret_cast<StepCounters *>(&ctx.ctrl->scalar[52]);
-    // delta_0 = the edges: rows are the CSR's values, units from its offsets
-    const u32 *rows = g.csr.val;
+    // delta_0 = the edges: one row per CSR value (its edge range), units from
+    // the CSR's offsets; the rows live in jbuf[1], the first step writes jbuf[0]
+    const uint2 *rows = nullptr;
     u64 nunits = 0, join = 0;
     DevBuf *ubuf = &ws.offsets, *ubuf_next = &ws.offsets_next;
     if (ne) {
@@ -551,6 +920,11 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         DL_LAUNCH(ctx, K_PREP, 16.0 * nunits,
                   units_fill_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, unit_rows, ws.w1.as<u64>(),
                                                                                      ubuf->as<Unit>()));
+        ctx.reserve(ws.jbuf[1], ne * 8);
+        DL_LAUNCH(ctx, K_PREP, 20.0 * ne,
+                  edge_rows_kernel<<<grid_for(ne, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, g.csr.val, ne,
+                                                                                     ws.jbuf[1].as<uint2>()));
+        rows = ws.jbuf[1].as<uint2>();
         DL_CUDA(cudaMemsetAsync(&ctr->join, 0, sizeof(u64), ctx.stream));
         DL_LAUNCH(ctx, K_PREP, 8.0 * ne,
                   edge_degree_sum_kernel<<<grid_for(ne, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, g.csr.val, ne,
@@ -578,26 +952,31 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         u64 nnew = 0, next_join = 0, next_units = 0;
         if (join) {
             pt.mark(PH_DEDUP);
+            const unsigned grid = (unsigned) std::min<u64>(nunits, resident);
+            // New rows <= join words. CTAs reserve rows in blocks of OCHUNK (a
+            // unit that overflows one continues in the next), so at most the
+            // last reservation of every CTA is left partly unused; unit slots
+            // are reserved UCHUNK at a time.
             DevBuf &obuf = ws.jbuf[slot];
-            ctx.reserve(obuf, join * 4);
-            const u64 ucap = nunits + join / unit_rows + 1;
+            const u64 ocap = join + (u64) grid * OCHUNK;
+            ctx.reserve(obuf, ocap * 8);
+            const u64 ucap = nunits + join / unit_rows + 1 + (u64) grid * UCHUNK;
             ctx.reserve(*ubuf_next, ucap * sizeof(Unit));
             DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(StepCounters), ctx.stream));
-            const unsigned grid = (unsigned) std::min<u64>(nunits, resident);
-            // algorithmic bytes: delta rows and units in, one edge target per join word, new rows and units out
-            DL_LAUNCH(ctx, K_BITMAP_EXPAND, 4.0 * nrows + 16.0 * nunits + 4.0 * join,
+            // algorithmic bytes: delta rows (8 B) and units in, one edge target per join word, new rows and units out
+            DL_LAUNCH(ctx, K_BITMAP_EXPAND, 8.0 * nrows + 16.0 * nunits + 4.0 * join,
                       kern<<<grid, UT, smem, ctx.stream>>>(g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m,
-                                                           stride, (u32) words_used, obuf.as<u32>(), join,
+                                                           stride, (u32) words_used, obuf.as<uint2>(), ocap,
                                                            ubuf_next->as<Unit>(), ucap, unit_rows,
                                                            ws.bit_hasout.as<u32>(), ctr, &ctx.ctrl->err));
             DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, ctr, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx.stream));
             ctx.sync();
-            const u64 next_rows = ctx.host_scalars[1];
+            const u64 next_rows = ctx.host_scalars[5];  // rows written (host_scalars[1]: rows reserved)
             next_join = ctx.host_scalars[2];
             next_units = ctx.host_scalars[3];
             nnew = ctx.host_scalars[4];
-            ctx.prof_add_bytes(K_BITMAP_EXPAND, 4.0 * next_rows + 16.0 * next_units);
-            rows = obuf.as<u32>();
+            ctx.prof_add_bytes(K_BITMAP_EXPAND, 8.0 * next_rows + 16.0 * next_units);
+            rows = obuf.as<uint2>();
             nrows = next_rows;
             slot ^= 1;
             std::swap(ubuf, ubuf_next);
@@ -651,7 +1030,136 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
     return nfull;
 }
 
+u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &opt, PhaseTimer &pt) {
+    Workspace &ws = ctx.ws;
+    const u64 n = g.n_ids;
+    const u64 stride = bitmat_stride(n);
+    const u64 unit_rows = std::max<u64>(1, ctx.tune.bitmap_unit_rows);
+    const u64 words_used = (n + 31) / 32;
+    const size_t smem = sizeof(SgSmem) + (3 * words_used + (words_used + 31) / 32) * 4 + 16;
+    if (smem > 227 * 1024) throw Error(DL_ERR_OUT_OF_MEMORY, "bit-matrix rows of " + std::to_string(n) +
+                                                              " nodes do not fit in shared memory");
+    DevBuf &M = ws.bitmat[0];
+    ctx.reserve(M, std::max<u64>(bitmat_bytes(n), 4));
+    DL_CUDA(cudaMemsetAsync(M.p, 0, bitmat_bytes(n), ctx.stream));
+    u32 *m = M.as<u32>();
+    StepCounters *ctr = reinterpret_cast<StepCounters *>(&ctx.ctrl->scalar[52]);
+    ctx.reserve(ws.bit_hasout, std::max<u64>(words_used, 1) * 4);
+    DL_LAUNCH(ctx, K_PREP, 4.0 * n + 4.0 * words_used,
+              hasout_kernel<<<grid_for(words_used, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, words_used,
+                                                                                      ws.bit_hasout.as<u32>()));
+    // base units (p, rows {p}) in offsets / jbuf[1]; the first step writes jbuf[0]
+    DevBuf *ubuf = &ws.offsets, *ubuf_next = &ws.offsets_next;
+    ctx.reserve(*ubuf, std::max<u64>(n, 1) * sizeof(Unit));
+    ctx.reserve(ws.jbuf[1], std::max<u64>(n, 1) * 8);
+    DL_CUDA(cudaMemsetAsync(&ctr->join, 0, sizeof(u64), ctx.stream));
+    DL_LAUNCH(ctx, K_PREP, 8.0 * n + 24.0 * n,
+              sg_base_units_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(
+                  g.csr.off, n, ws.jbuf[1].as<uint2>(), ubuf->as<Unit>(), &ctr->join));
+    DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, &ctr->join, sizeof(u64), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    u64 bound = ctx.host_scalars[0];
+    const uint2 *rows = ws.jbuf[1].as<uint2>();
+    u64 nunits = n, nrows = n;
+    auto kern = sg_unit_step_kernel;
+    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int per_sm = 0;
+    DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, UT, smem));
+    const u64 resident = (u64) ctx.sm_count * std::max(per_sm, 1);
+    u64 nfull = 0;
+    int slot = 0;
+    for (int it = 0;; ++it) {  // it 0: the base rule (sg.cu:170-217); then sg.cu:244-390
+        pt.mark(it == 0 ? PH_INIT : PH_JOIN);
+        u64 nnew = 0, next_units = 0, next_rows = 0, next_bound = 0;
+        if (nunits && bound) {
+            const unsigned grid = (unsigned) std::min<u64>(nunits, resident);
+            const u64 warps = (u64) grid * UW;
+            // New rows < bound; a warp's reservations are at least 3/4 used
+            // (a switch leaves less than one summary word's rows, <= 1024,
+            // behind). The buffer is also capped by the device memory left; a
+            // step that overflows it reports DL_DEVERR_CAPACITY and the caller
+            // reruns the program on the sorted runs.
+            size_t free_b = 0, total_b = 0;
+            DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            const u64 need = bound + bound / 3 + warps * WCHUNK;
+            // rows (8 B) at most 1/16 of the free memory, unit slots (16 B, at
+            // most one per row) at most 1/8
+            const u64 cap_rows = std::max<u64>(warps * WCHUNK, (u64) free_b / 16 / 8);
+            const u64 ocap = std::min(need, cap_rows);
+            DevBuf &obuf = ws.jbuf[slot];
+            ctx.reserve(obuf, ocap * 8);
+            const u64 ucap = ocap + warps * UCHUNK;  // every unit written holds at least one row
+            ctx.reserve(*ubuf_next, ucap * sizeof(Unit));
+            DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(StepCounters), ctx.stream));
+            pt.mark(PH_DEDUP);
+            DL_LAUNCH(ctx, K_BITMAP_EXPAND, 8.0 * nrows + 16.0 * nunits,
+                      kern<<<grid, UT, smem, ctx.stream>>>(g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m,
+                                                           stride, (u32) words_used, obuf.as<uint2>(), ocap,
+                                                           ubuf_next->as<Unit>(), ucap, unit_rows,
+                                                           ws.bit_hasout.as<u32>(), ctr, &ctx.ctrl->err,
+                                                           it == 0 ? 1 : 0));
+            DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, ctr, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx.stream));
+            ctx.sync();  // a capacity overflow throws DL_ERR_OVERFLOW here
+            next_rows = ctx.host_scalars[5];
+            next_bound = ctx.host_scalars[2];
+            next_units = ctx.host_scalars[3];
+            nnew = ctx.host_scalars[4];
+            ctx.prof_add_bytes(K_BITMAP_EXPAND, 8.0 * next_rows + 16.0 * next_units);
+            rows = obuf.as<uint2>();
+            slot ^= 1;
+            std::swap(ubuf, ubuf_next);
+        }
+        pt.mark(PH_MERGE);
+        nfull += nnew;
+        if (it > 0) {
+            r.deltas.push_back((i64) nnew);
+            r.joins.push_back((i64) nrows);
+            r.fulls.push_back((i64) nfull);
+        }
+        nunits = next_units;
+        nrows = next_rows;
+        bound = next_bound;
+        if (it > 0 && nnew == 0) break;  // |full| unchanged
+        if (it > 0 && opt.max_iterations > 0 && it >= opt.max_iterations) break;
+    }
+    pt.mark(PH_FINAL);
+    // result rows in the reference's SG order (x, y) by (x, y): straight from
+    // M's rows when they are copied out
+    if (nfull) {
+        ctx.reserve(ws.offsets, (n + 1) * 8);
+        u64 *counts = ws.offsets.as<u64>();
+        DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 4.0 * n * words_used,
+                  bitmat_row_popc_kernel<<<grid_for(n * 32, T256, ctx, 8), T256, 0, ctx.stream>>>(
+                      m, n, stride, words_used, reinterpret_cast<unsigned long long *>(counts)));
+        ctx.reserve(ws.w0, (n + 1) * 8);
+        const u64 total = exclusive_scan(ctx, counts, n, ws.w0.as<u64>());
+        if (total != nfull)
+            throw Error(DL_ERR_INTERNAL, "bit matrix holds " + std::to_string(total) + " tuples, expected " +
+                                             std::to_string(nfull));
+        r.bm_t = M;
+        M = DevBuf();
+        r.bm_first = ws.w0;
+        ws.w0 = DevBuf();
+        r.bm_n = n;
+        r.bm_stride = stride;
+        r.bm_words = words_used;
+        r.bm_row_first = true;
+    }
+    r.from_bitmat = true;
+    return nfull;
+}
+
 }  // namespace detail
+
+// One wave of the extraction kernel (every CTA resident at once; rows are
+// strided over them), so no partial second wave runs at low occupancy.
+static unsigned extract_grid(Context &ctx, u64 n) {
+    using namespace detail;
+    int per_sm = 0;
+    DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bitmat_extract_rows_kernel<false>, EX_THREADS, 0));
+    const u64 wave = (u64) ctx.sm_count * std::max(per_sm, 1);
+    return (unsigned) std::max<u64>(1, std::min<u64>(wave, (n + EX_THREADS / 32 - 1) / (EX_THREADS / 32)));
+}
 
 // The result rows of a bit-matrix TC run, written straight from the stored
 // transpose into `out` (device memory): (x, z) rows ordered by (z, x).
@@ -659,10 +1167,17 @@ void bitmat_extract_rows(Context &ctx, const Run &r, int32_t *out) {
     using namespace detail;
     if (r.info.output_rows == 0) return;
     const u64 n = r.bm_n;
-    DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 4.0 * n * r.bm_words + 8.0 * (double) r.info.output_rows,
-              bitmat_extract_rows_kernel<<<grid_for(n * 32, EX_THREADS, ctx, 8), EX_THREADS, 0, ctx.stream>>>(
-                  r.bm_t.as<u32>(), n, r.bm_stride, r.bm_words, r.bm_first.as<u64>(), r.ids.as<int32_t>(),
-                  reinterpret_cast<u64 *>(out)));
+    const double bytes = 4.0 * n * r.bm_words + 8.0 * (double) r.info.output_rows;
+    if (r.bm_row_first)
+        DL_LAUNCH(ctx, K_BITMAP_EXTRACT, bytes,
+                  bitmat_extract_rows_kernel<true><<<extract_grid(ctx, n), EX_THREADS, 0, ctx.stream>>>(
+                      r.bm_t.as<u32>(), n, r.bm_stride, r.bm_words, r.bm_first.as<u64>(), r.ids.as<int32_t>(),
+                      r.ids_affine, r.id_base, reinterpret_cast<u64 *>(out)));
+    else
+        DL_LAUNCH(ctx, K_BITMAP_EXTRACT, bytes,
+                  bitmat_extract_rows_kernel<false><<<extract_grid(ctx, n), EX_THREADS, 0, ctx.stream>>>(
+                      r.bm_t.as<u32>(), n, r.bm_stride, r.bm_words, r.bm_first.as<u64>(), r.ids.as<int32_t>(),
+                      r.ids_affine, r.id_base, reinterpret_cast<u64 *>(out)));
 }
 
 }  // namespace dl

@@ -276,6 +276,18 @@ DL_API dl_status dl_remove_self_pairs(dl_context *ctx, dl_entity *rel, int64_t n
     });
 }
 
+DL_API dl_status dl_partition(dl_context *ctx, const dl_entity *rel, int64_t n, int32_t ranks, int32_t swap_columns,
+                              dl_entity *out, int64_t *counts) {
+    DL_REQUIRE(ctx && counts && n >= 0 && (n == 0 || (rel && out && (const void *) rel != (const void *) out)) &&
+                   ranks >= 1 && (u64) ranks <= dl::kMaxPartitionRanks,
+               "invalid argument");
+    return guarded([&] {
+        set_device(ctx);
+        dl::partition_rows(ctx->c, (const int32_t *) rel, (u64) n, (uint32_t) ranks, swap_columns != 0, (int32_t *) out,
+                           counts);
+    });
+}
+
 DL_API dl_status dl_build_hash_table(dl_context *ctx, const dl_entity *rel, int64_t n, double load_factor,
                                      dl_hash_table **out) {
     DL_REQUIRE(ctx && out && n >= 0 && (rel || n == 0), "invalid argument");
@@ -624,6 +636,7 @@ DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out) {
     out->hash_load_factor = t.hash_load;
     out->bitmap_max_gib = t.bitmap_max_gib;
     out->bitmap_unit_rows = (int32_t) t.bitmap_unit_rows;
+    out->cache_max_gib = t.cache_max_gib;
     return DL_OK;
 }
 
@@ -639,6 +652,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     DL_REQUIRE(t->hash_load_factor > 0.0 && t->hash_load_factor < 1.0, "hash_load_factor must be in (0, 1)");
     DL_REQUIRE(t->bitmap_max_gib >= 0 && t->bitmap_max_gib <= 1024, "bitmap_max_gib must be in 0..1024");
     DL_REQUIRE(t->bitmap_unit_rows >= 1 && t->bitmap_unit_rows <= (1 << 24), "bitmap_unit_rows must be in 1..16777216");
+    DL_REQUIRE(t->cache_max_gib >= 0 && t->cache_max_gib <= 1024, "cache_max_gib must be in 0..1024");
     dl::Tuning &o = ctx->c.tune;
     o.sort_algo = t->sort_algorithm;
     o.rank = t->sort_ranking;
@@ -650,6 +664,8 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     o.hash_load = t->hash_load_factor;
     o.bitmap_max_gib = t->bitmap_max_gib;
     o.bitmap_unit_rows = (uint32_t) t->bitmap_unit_rows;
+    o.cache_max_gib = t->cache_max_gib;
+    ctx->c.trim_spares();
     return DL_OK;
 }
 

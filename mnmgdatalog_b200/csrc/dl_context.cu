@@ -93,11 +93,12 @@ void Context::allocate(DevBuf &buf, size_t bytes, bool zero, size_t minimum) {
 }
 
 void Context::trim_spares() {
-    // Cache at most kSpareCount buffers and kSpareBytes in total, freeing the
+    // Cache at most kSpareCount buffers and tune.cache_max_gib in total, freeing the
     // smallest first (large buffers are the expensive ones to re-create).
     size_t total = 0;
     for (const auto &s : spares) total += s.cap;
-    while (spares.size() > kSpareCount || total > kSpareBytes) {
+    const size_t limit = (size_t) tune.cache_max_gib << 30;
+    while (!spares.empty() && (spares.size() > kSpareCount || total > limit)) {
         int small = 0;
         for (int i = 1; i < (int) spares.size(); ++i)
             if (spares[i].cap < spares[small].cap) small = i;
@@ -160,6 +161,7 @@ void Context::check_device_error() {
         DL_CUDA(cudaStreamSynchronize(stream));
         reinterpret_cast<volatile u32 *>(host_scalars)[2 * 63] = 0;
         if (err & DL_DEVERR_HASH_FULL) throw Error(DL_ERR_INTERNAL, "hash set probe sequence exceeded its capacity");
+        if (err & DL_DEVERR_CAPACITY) throw Error(DL_ERR_OVERFLOW, "a device buffer was smaller than its contents");
         if (err & DL_DEVERR_LOOKBACK)
             throw Error(DL_ERR_DEVICE_TIMEOUT, "a device-side wait exceeded its limit (decoupled look-back)");
         throw Error(DL_ERR_INTERNAL, "device error flag " + std::to_string(err));

@@ -176,6 +176,32 @@ void rank_nodes(Context &ctx, const int32_t *rows, u64 n, Graph &g) {
     g.ids = ws.ids.as<int32_t>();
 }
 
+__global__ void id_range_kernel(int32_t *__restrict__ ids, u64 n, int32_t base) {
+    GRID_STRIDE(i, n) ids[i] = (int32_t) ((int64_t) base + (int64_t) i);
+}
+
+template <class Fits>
+bool densify_ids(Context &ctx, Graph &g, Fits fits) {
+    if (g.n_ids == 0) return false;
+    int32_t ends[2];
+    DL_CUDA(cudaMemcpyAsync(&ends[0], g.ids, 4, cudaMemcpyDeviceToHost, ctx.stream));
+    DL_CUDA(cudaMemcpyAsync(&ends[1], g.ids + g.n_ids - 1, 4, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.sync();
+    const u64 range = (u64) ((int64_t) ends[1] - (int64_t) ends[0]) + 1;
+    if (range > (u64) g.n_ids + g.n_ids / 8 || range > 0x7FFFFFFFull || !fits(range)) return false;
+    Workspace &ws = ctx.ws;
+    ctx.reserve(ws.ids, range * 4);
+    DL_LAUNCH(ctx, K_PREP, 4.0 * range,
+              id_range_kernel<<<grid_for(range, T256, ctx), T256, 0, ctx.stream>>>(ws.ids.as<int32_t>(), range,
+                                                                                  ends[0]));
+    g.n_ids = (u32) range;
+    g.bits = bits_for(range);
+    g.ids = ws.ids.as<int32_t>();
+    g.ids_affine = true;
+    g.id_base = ends[0];
+    return true;
+}
+
 // Sorted, duplicate-free words (key rank << bits | value rank) -> CSR.
 void build_csr(Context &ctx, const u64 *words, u64 n, Graph &g) {
     Workspace &ws = ctx.ws;
@@ -311,6 +337,8 @@ void adopt_ids(Context &ctx, Run &r, const Graph &g) {
     r.n_ids = g.n_ids;
     r.bits = g.bits;
     r.info.nodes = g.n_ids;
+    r.ids_affine = g.ids_affine;
+    r.id_base = g.id_base;
 }
 
 // The full relation of TC/SG as disjoint sorted duplicate-free runs: a large
@@ -459,6 +487,15 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     F.three = true;  // plain runs: large, small and tiny runs
     if (n > 0) {
         rank_nodes(ctx, rows, n, g);
+        // On the bit-matrix path, a dense id range is ranked as is: the
+        // result rows then need no rank -> id table lookups.
+        const bool dense = densify_ids(ctx, g, [&](u64 range) {
+            try {
+                return bitmat_choose(ctx, opt, range, 2);
+            } catch (const Error &) {  // a forced bit matrix that fits only without the absent ids
+                return false;
+            }
+        });
         ctx.reserve(ws.jbuf[0], n * 8);
         ctx.reserve(ws.jbuf[1], n * 8);
         DL_LAUNCH(ctx, K_PREP, 0, pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
@@ -466,7 +503,7 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         u64 ne;
         u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, n, 2 * g.bits, ne);
         build_csr(ctx, e, ne, g);
-        if (bitmat_choose(ctx, opt, g.n_ids)) {
+        if (dense || bitmat_choose(ctx, opt, g.n_ids, 2)) {
             nfull = tc_bitmap_fixpoint(ctx, r, g, e, ne, opt, pt);  // result: the transpose, in r
             cur = 0;
         } else {
@@ -580,6 +617,17 @@ static void run_tc_hash_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n
 
 // SG (sg.cu:40-477): base sg(x,y) :- e(p,x), e(p,y), x != y; recursive rule
 // as two joins with the column swaps fused into the emit.
+// SG's edge relation: the input rows as sorted duplicate-free words (in
+// jbuf[0] or jbuf[1]).
+static u64 *sg_edge_words(Context &ctx, const int32_t *rows, u64 n, const Graph &g, u64 &ne) {
+    Workspace &ws = ctx.ws;
+    ctx.reserve(ws.jbuf[0], n * 8);
+    ctx.reserve(ws.jbuf[1], n * 8);
+    DL_LAUNCH(ctx, K_PREP, 0, pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
+                                                                     ws.jbuf[0].as<u64>(), nullptr));
+    return sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * g.bits, ne);
+}
+
 static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, bool on_device, const dl_options &opt) {
     Workspace &ws = ctx.ws;
     PhaseTimer pt(ctx, opt.phase_timing != 0);
@@ -592,15 +640,41 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     int cur = 0;
     FullSet F;
     F.three = true;  // plain runs: large, small and tiny runs
+    bool on_bitmat = false;
     if (n > 0) {
         rank_nodes(ctx, rows, n, g);
-        ctx.reserve(ws.jbuf[0], n * 8);
-        ctx.reserve(ws.jbuf[1], n * 8);
-        DL_LAUNCH(ctx, K_PREP, 0, pack_rows_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(rows, n, g.ids, g.n_ids, g.bits,
-                                                                         ws.jbuf[0].as<u64>(), nullptr));
+        // As for TC: a dense id range is ranked as is when the bit matrix is used.
+        const bool dense = densify_ids(ctx, g, [&](u64 range) {
+            try {
+                return bitmat_choose(ctx, opt, range, 1);
+            } catch (const Error &) {
+                return false;
+            }
+        });
         u64 ne;
-        u64 *e = sort_unique_into(ctx, ws.jbuf[0], ws.jbuf[1], n, 2 * g.bits, ne);  // sg.cu:150-153
-        build_csr(ctx, e, ne, g);                                                    // sg.cu:162
+        u64 *e = sg_edge_words(ctx, rows, n, g, ne);  // sg.cu:150-153
+        build_csr(ctx, e, ne, g);                     // sg.cu:162
+        if (dense || bitmat_choose(ctx, opt, g.n_ids, 1)) {
+            try {
+                nfull = sg_bitmap_fixpoint(ctx, r, g, opt, pt);
+                on_bitmat = true;
+            } catch (const Error &err) {
+                if (err.status != DL_ERR_OVERFLOW) throw;
+                // a step outgrew the memory left for its new rows: the sorted runs
+                // need no such bound; start over on them (same graph)
+                r.deltas.clear();
+                r.joins.clear();
+                r.fulls.clear();
+                r.from_bitmat = false;
+                ctx.give_back(r.bm_t);
+                ctx.give_back(r.bm_first);
+                nfull = 0;
+            }
+        }
+    }
+    if (n > 0 && !on_bitmat) {
+        u64 ne;
+        u64 *e = sg_edge_words(ctx, rows, n, g, ne);  // again: the bit-matrix attempt reused the buffers
         // Base rule (sg.cu:170-217): probe = deduplicated edges.
         u64 *selfs = &ctx.ctrl->scalar[8];
         DL_CUDA(cudaMemsetAsync(selfs, 0, sizeof(u64), ctx.stream));
@@ -641,9 +715,11 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
     DL_CUDA(cudaEventRecord(ev.b, ctx.stream));
     pt.mark(PH_FINAL);
     adopt_ids(ctx, r, g);
-    r.words = ws.full[cur];
-    ws.full[cur] = DevBuf();
-    r.n_words = nfull;
+    if (!on_bitmat) {
+        r.words = ws.full[cur];
+        ws.full[cur] = DevBuf();
+        r.n_words = nfull;
+    }
     r.info.output_rows = r.info.output_tuples = (i64) nfull;
     finish_info(r, ctx, ev.a, ev.b, pt);
 }

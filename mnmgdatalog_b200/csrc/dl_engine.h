@@ -16,14 +16,17 @@ struct Run {
     u64 n_words = 0;
     DevBuf ids;               // node id of each rank
     u32 n_ids = 0;
+    bool ids_affine = false;  // ids[r] == id_base + r
+    int32_t id_base = 0;
     int bits = 1;             // bits per rank in a word
     DevBuf aux;               // WCC: component ranks, ascending
     u64 n_aux = 0;
     DevBuf labels;            // WCC: label rank of every node
-    // TC on the bit matrix: the result stays as the matrix's transpose (row =
-    // path target) and each row's first output position; rows are extracted
-    // when they are copied out
+    // TC / SG on the bit matrix: the result stays as the matrix's transpose
+    // (TC: row = path target) or the matrix (SG) with each row's first output
+    // position; rows are extracted when they are copied out
     bool from_bitmat = false;
+    bool bm_row_first = false;  // SG: the matrix itself, rows (row id, column id)
     DevBuf bm_t, bm_first;
     u64 bm_n = 0, bm_stride = 0, bm_words = 0;
 };

@@ -51,6 +51,9 @@ struct Graph {
     u32 n_ids = 0;
     int bits = 1;
     int32_t *ids = nullptr;
+    // ids[r] == id_base + r for every rank (the ranks cover a dense id range)
+    bool ids_affine = false;
+    int32_t id_base = 0;
     Csr csr;
     // Radix windows of join-output sorts; 0 = every digit of [0, 2 * bits).
     int nwin = 0;
@@ -77,6 +80,12 @@ struct FullSet {
 
 
 int bits_for(u64 n);
+// Ranks over every id in [min id, max id] when that range is at most 1/8
+// larger than the distinct ids (absent ids become ranks without edges):
+// rank -> id is then id_base + rank, with no table lookup. Returns whether
+// it did; `fits(range)` decides whether the caller can use that many ranks.
+template <class Fits>
+bool densify_ids(Context &ctx, Graph &g, Fits fits);
 const int32_t *stage_input(Context &ctx, const int32_t *rows, u64 n, bool on_device);
 void rank_nodes(Context &ctx, const int32_t *rows, u64 n, Graph &g);
 u64 *sort_unique_into(Context &ctx, DevBuf &buf, DevBuf &alt, u64 n, int key_bits, u64 &n_out);
@@ -92,9 +101,15 @@ void settle(Context &ctx, FullSet &F);
 
 // TC with full as an n x n bit matrix (dl_bitmap.cu).
 u64 bitmat_bytes(u64 n);
-bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n);
+// Whether a run over n node ranks keeps full as an n x n bit matrix:
+// `copies` matrices (TC 2: the matrix and its transpose; SG 1) must fit.
+bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, int copies);
 u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u64 ne, const dl_options &opt,
                        PhaseTimer &pt);
+// SG with full as a bit matrix; throws DL_ERR_OVERFLOW when a step's new rows
+// outgrow the buffer the device memory allows (the caller then reruns SG on
+// the sorted runs).
+u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &opt, PhaseTimer &pt);
 
 }  // namespace detail
 }  // namespace dl

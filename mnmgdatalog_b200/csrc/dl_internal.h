@@ -128,6 +128,7 @@ struct Tuning {
     double hash_load = 0.5;     // default load factor of dl_build_hash_table
     int bitmap_max_gib = 48;    // TC dedup AUTO: bit matrix and transpose at most this many GiB (0 = never)
     u32 bitmap_unit_rows = 65536;  // bit-matrix TC: delta rows per unit (one shared-memory row fold each)
+    int cache_max_gib = 96;        // cached spare buffers of the context, at most this many GiB
 };
 Tuning default_tuning();
 
@@ -154,8 +155,7 @@ struct Context {
     // Freeing a multi-GB buffer costs milliseconds and synchronises the
     // device, so outgrown buffers stay cached; an allocation that fails
     // drops the whole cache and retries (Context::allocate).
-    static constexpr size_t kSpareCount = 256;
-    static constexpr size_t kSpareBytes = 96ull << 30;
+    static constexpr size_t kSpareCount = 256;  // and at most tune.cache_max_gib GiB
 
     // Live profile: every launch is counted; with prof_on each launch is
     // bracketed by events that are resolved at the next sync().

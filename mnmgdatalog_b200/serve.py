@@ -127,7 +127,8 @@ class Server:
 
     def __init__(self, engine=None, *, budget_bytes: int = 150 * 10**9, wcc_stop: str = "reference",
                  max_active: int = 0, backend=None, clock=time.perf_counter, keep_results: bool = True,
-                 concurrent: bool = False, output: str = "host", pinned: bool = False, tuning: dict | None = None):
+                 concurrent: bool = False, output: str = "host", pinned: bool = False, tuning: dict | None = None,
+                 cache_gib: int = 4):
         self.budget = int(budget_bytes)
         self.output = output  # where result rows go: "host" (delivered), "device" or "none"
         self.pool = PinnedPool() if (pinned and output == "host") else None
@@ -146,6 +147,9 @@ class Server:
                     e = Engine(engine.device)
                     if tuning:
                         e.set_tuning(tuning)
+                    # buffers a worker keeps for reuse are outside the budget's
+                    # accounting: keep them small next to the other workers
+                    e.set_tuning(cache_max_gib=cache_gib)
                     self._engines.append(e)
                     backend[p] = (lambda p=p, e=e: e.session(p, wcc_stop=wcc_stop))
             else:
@@ -435,13 +439,27 @@ def poisson_arrivals(count: int, rate: float, rng: np.random.Generator) -> np.nd
     return np.cumsum(rng.exponential(1.0 / rate, size=count))
 
 
+def relabel(edges: np.ndarray, seed: int) -> np.ndarray:
+    """The same graph under a seeded injective map of node ids,
+    id -> (a * id + b) mod (2^31 - 1) (a prime modulus, a != 0): a distinct
+    input with the same structure, the same closure sizes and different
+    result rows. Ids stay in [0, 2^31 - 2], so never the reference's -1."""
+    P = 2**31 - 1
+    rng = np.random.default_rng(seed)
+    a = int(rng.integers(1, P))
+    b = int(rng.integers(0, P))
+    e = np.asarray(edges, dtype=np.int64)
+    return ((e * a + b) % P).astype(np.int32)
+
+
 def mixed_requests(count: int, *, lo: int = 1000, hi: int = 500_000, pool: int = 48, seed: int = 0,
-                   programs=PROGRAMS) -> list[Request]:
+                   programs=PROGRAMS, distinct: bool = False) -> list[Request]:
     """A mixed TC/SG/WCC request list: programs uniform, edge counts
-    log-uniform in [lo, hi]. Inputs are drawn from a pool of `pool` seeded
-    graphs per program (generating every request's graph afresh would take
-    longer than serving it); the server keeps no result cache, so a repeated
-    input is computed again like any other."""
+    log-uniform in [lo, hi]. Inputs come from a pool of `pool` seeded graphs
+    per program (generating every request's graph afresh would take longer
+    than serving it); with `distinct`, every request relabels its pool graph
+    by its own seeded id map (relabel), so no two requests carry the same
+    input. The server keeps no result cache either way."""
     from . import graphs
     rng = np.random.default_rng(seed)
     bank = {}
@@ -451,7 +469,8 @@ def mixed_requests(count: int, *, lo: int = 1000, hi: int = 500_000, pool: int =
     out = []
     for i in range(count):
         p = programs[int(rng.integers(len(programs)))]
-        out.append(Request(i, p, bank[p][int(rng.integers(pool))]))
+        e = bank[p][int(rng.integers(pool))]
+        out.append(Request(i, p, relabel(e, seed * 1_000_003 + i) if distinct else e))
     return out
 
 

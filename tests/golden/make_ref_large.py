@@ -53,9 +53,16 @@ CASES = [
     ("ego_facebook_sg", "sg", "data_88234.bin", (15_018_986, 13), "logs/small-merged-job-output.txt:269"),
     ("fe_ocean_sg", "sg", "data_409593.bin", (65_941_441, 77), "README.md:54"),
     ("c1_tc_chung_lu", "tc", "synthetic:c1_tc_chung_lu", None, None),
+    # single_join's synthetic rows (glibc srand(1)/rand(), common/parallel_io.cu:79-108): the weak- and
+    # strong-scaling inputs of one rank; the reference never writes this program's output file (job_run
+    # is fixed at 1, single_join.cu:78), so these are pinned by counts
+    ("single_join_weak", "single_join", "rows:10000000:500000", (199_915_594, 1),
+     "drawing/charts/single_join_weak (copy).csv:2"),
+    ("single_join_strong", "single_join", "rows:10000001:100000", (1_037_050_773, 1),
+     "drawing/charts/single_join_strong (copy).csv:2"),
 ]
 
-LARGE_FILES = sorted({c[2] for c in CASES if not c[2].startswith("synthetic:")})
+LARGE_FILES = sorted({c[2] for c in CASES if not c[2].startswith(("synthetic:", "rows:"))})
 INT_MAX = 2**31 - 1
 
 
@@ -65,6 +72,10 @@ def load_case_input(name: str) -> np.ndarray:
     if name.startswith("synthetic:"):
         from mnmgdatalog_b200 import graphs
         return graphs.make(name.split(":", 1)[1], seed=0)[1]
+    if name.startswith("rows:"):  # single_join rows: (count, rand_range) through the library's generator
+        from mnmgdatalog_b200 import generate_rows
+        _, rows, rng = name.split(":")
+        return generate_rows(int(rows), int(rng), 1)
     with gzip.open(os.path.join(HERE, "data", name + ".gz"), "rb") as f:
         raw = f.read()
     return np.frombuffer(raw, dtype="<i4")[: (len(raw) // 8) * 2].reshape(-1, 2).copy()
@@ -105,8 +116,26 @@ def run(out_path: str, only: list[str], timeout: int) -> None:
     for case, prog, inp, published, cite in CASES:
         if only and case not in only:
             continue
-        edges = load_case_input(inp)
         binary = os.path.join(refdir, f"{prog}.out")
+        if prog == "single_join":  # generates its own rows: argv = rows, cuda_aware, comm_method, rand_range
+            _, rows, rng = inp.split(":")
+            t0 = time.perf_counter()
+            r = subprocess.run([binary, rows, "0", "0", rng], capture_output=True, text=True, timeout=timeout)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                raise SystemExit(f"{case}: {binary} exited {r.returncode}\n{r.stderr[-2000:]}")
+            csv = [l for l in r.stdout.splitlines() if l and l[0].isdigit()][-1].split(",")
+            results[case] = {"program": prog, "input": inp, "input_rows": int(csv[0]), "iterations": 1,
+                             "tuples": int(csv[3]), "reference_total_s": float(csv[4]), "wall_s": round(wall, 2),
+                             "published": list(published), "published_source": cite,
+                             "command": f"oracle/_ref/single_join.out {rows} 0 0 {rng}", "rows_sha256": None,
+                             "rows_note": "the reference does not write this output (job_run = 1, single_join.cu:78)"}
+            print(case, results[case]["tuples"], results[case]["reference_total_s"], flush=True)
+            with open(out_path, "w") as f:
+                json.dump({"generator": "tests/golden/make_ref_large.py run", "cases": results}, f, indent=1,
+                          sort_keys=True)
+            continue
+        edges = load_case_input(inp)
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "input.bin")
             edges.astype("<i4").tofile(path)

@@ -8,7 +8,10 @@ output file (rows in the reference's file order). Every case is also checked
 against the count the reference published for that input. TC runs on both of
 the engine's dedup paths (the bit matrix and the sorted runs); where the
 reference cannot write its output (2^31 or more int32 values), the two paths'
-rows are compared with each other instead.
+rows are compared with each other instead; single_join's output the
+reference never writes (job_run is fixed at 1, single_join.cu:78), so its
+weak- and strong-scaling inputs are pinned by counts (rows are compared with
+the oracle at smaller sizes in test_programs_gpu.py).
 """
 import hashlib
 import json
@@ -79,9 +82,10 @@ def test_counts_equal_reference_and_paths_agree(engine, case):
     shas = {}
     modes = ["auto", "sort"] if ref["program"] == "tc" else ["auto"]
     for dedup in modes:
-        r = engine.run(ref["program"], edges, dedup=dedup)
+        r = engine.run(ref["program"], edges, dedup=dedup, output="host" if len(modes) > 1 else "none")
         _check_counts(case, r)
-        shas[dedup] = _sha(r.rows)
+        if len(modes) > 1:
+            shas[dedup] = _sha(r.rows)
         del r
-    assert len(set(shas.values())) == 1, shas
+    assert len(set(shas.values())) <= 1, shas
     engine.release_memory()
