@@ -54,6 +54,8 @@ def _env_int(k, d):
 
 
 def workload(config: str):
+    if config == "sg_fe_body":  # the reference's fe_body input (data/data_163734.bin)
+        return "sg", load_fixture(SG_DATASET[0])
     from mnmgdatalog_b200 import graphs
     prog, edges = graphs.make(config, seed=0)
     return prog, edges
@@ -64,7 +66,8 @@ def describe(config: str, edges: np.ndarray) -> dict:
          "c0_tc_dag": "TC, DAG n=5000 p=0.7 + 2000 short edges (seed 0)",
          "c2_sg_lattice": "SG, 55^3 lattice 6-neighbour p=0.15 + 1% long edges (seed 0)",
          "p1_tc_chung_lu_small": "TC, Chung-Lu n=40000 gamma=2.5 m=132500 (each edge once, seed 0)",
-         "p2_tc_chung_lu_medium": "TC, Chung-Lu n=80000 gamma=2.5 m=265000 (each edge once, seed 0)"}
+         "p2_tc_chung_lu_medium": "TC, Chung-Lu n=80000 gamma=2.5 m=265000 (each edge once, seed 0)",
+         "sg_fe_body": "SG, the reference's fe_body input (data/data_163734.bin, 163,734 edges)"}
     return {"workload": d.get(config, config), "config": config, "input_rows": int(len(edges))}
 
 

@@ -216,3 +216,25 @@ def test_tc_bitmap_max_iterations_and_selection(engine):
             assert np.array_equal(r.rows, engine.tc(e, dedup="sort").rows)
     finally:
         engine.set_tuning(before)
+
+
+@pytest.mark.parametrize("unit_rows", [1, 7, 65536])
+def test_sg_bitmap_agrees_with_sorted_runs(engine, unit_rows):
+    """SG on the bit matrix (the base rule's units (p, {p}), one fold per
+    out-edge of a unit's source) against SG on the sorted runs, with delta
+    units split into 1, 7 or up to 65,536 rows: the same iterations, deltas
+    and rows."""
+    from mnmgdatalog_b200 import graphs
+    before = engine.tuning()
+    inputs = [graphs.lattice3d(side=14, p=0.3, seed=5), graphs.chung_lu(n=3000, m=8000, seed=3),
+              graphs.dag(n=1500, extra=500, seed=2)]
+    inputs += [load_input(f) for f in ("data_10.bin", "hipc_2019.bin", "data_7035.bin", "quiz3.bin")]
+    try:
+        engine.set_tuning(bitmap_unit_rows=unit_rows)
+        for k, e in enumerate(inputs):
+            a = engine.sg(e, dedup="sort")
+            b = engine.sg(e, dedup="bitmap")
+            assert a.iterations == b.iterations and a.deltas.tolist() == b.deltas.tolist(), k
+            assert np.array_equal(a.rows, b.rows), k
+    finally:
+        engine.set_tuning(before)
