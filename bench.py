@@ -414,13 +414,13 @@ def load_fixture(name: str) -> np.ndarray:
     return np.frombuffer(raw, dtype="<i4")[: (len(raw) // 8) * 2].reshape(-1, 2).copy()
 
 
-SINGLE_JOIN = (10_000_001, 100_000, 1_037_050_773, "drawing/charts/single_join_strong (copy).csv:2")
+SINGLE_JOIN = (10_000_001, 90_000, 1_037_050_773, "logs/single-join-small-job-output.txt:104-106")
 
 
 def measure_single_join(eng, args, dev, flush) -> dict:
     """single_join's strong-scaling input on one GPU: 10,000,001 rows of
-    glibc srand(1)/rand() values in [1, 100,000] (the reference published
-    1,037,050,773 output rows, 1.78 s on an A100), timed like the main leg,
+    glibc srand(1)/rand() values in [1, 90,000] (the reference published
+    1,037,050,773 output rows for it on one A100), timed like the main leg,
     with the reference's own GPU program on the same rows."""
     import torch
 
@@ -449,7 +449,9 @@ def measure_single_join(eng, args, dev, flush) -> dict:
                         f"published {pub} output rows, {cite})",
             "value": res.output_tuples * steps / (sum(ms) / 1e3), "unit": UNIT, "steps": steps,
             "ms_per_step": sum(ms) / steps, "tuples": int(res.output_tuples),
-            "matches_published": bool(res.output_tuples == pub), "roofline": roofline, "kernels": kernels,
+            "matches_published": bool(res.output_tuples == pub),
+            "matches_reference": (bool(res.output_tuples == ref["tuples"]) if ref and "tuples" in ref else None),
+            "roofline": roofline, "kernels": kernels,
             "gpu_launches": launches, "reference_gpu": ref}
 
 
@@ -605,6 +607,7 @@ def measure_served(eng, args, tuning=None) -> dict:
     sample = reqs[::every]
     t_plain, svc, _ = serve.serve_plain(eng, sample, pinned=True, keep_results=False)
     eng.set_tuning(before)
+    eng.release_memory()  # the plain engine's cached buffers would crowd the server's budget
     plain_qps = len(sample) / t_plain
 
     def fresh():

@@ -96,12 +96,14 @@ constexpr u32 SCHUNK = 8;        // summary words per warp chunk in the fold and
 constexpr u64 OCHUNK = 1 << 18;  // next-delta rows a CTA reserves at a time (a unit crossing the end of one is split)
 constexpr u64 UCHUNK = 16;       // next-delta unit slots a CTA reserves at a time
 
-// Shared memory of the expansion of a unit's rows into a shared row.
-struct ExpandSmem {
-    u32 wbeg[UW][32];   // per-warp compacted rows: first edge
-    u32 wdeg[UW][32];   // and degree
+// Shared memory of the expansion of a unit's rows into a shared row (NW warps).
+template <int NW>
+struct ExpandSmemT {
+    u32 wbeg[NW][32];   // per-warp compacted rows: first edge
+    u32 wdeg[NW][32];   // and degree
     u32 next_group;     // next row group to take
 };
+using ExpandSmem = ExpandSmemT<UW>;
 
 struct UnitSmem {
     ExpandSmem e;
@@ -139,7 +141,8 @@ __global__ void hasout_kernel(const u32 *__restrict__ off, u64 n, u64 words, u32
 }
 
 // Next row group of the unit for this warp (lane 0 takes it, all lanes get it).
-__device__ __forceinline__ u32 take_group(ExpandSmem &s, u32 lane) {
+template <int NW>
+__device__ __forceinline__ u32 take_group(ExpandSmemT<NW> &s, u32 lane) {
     u32 g = 0;
     if (lane == 0) g = atomicAdd(&s.next_group, 1u);
     return __shfl_sync(0xffffffffu, g, 0);
@@ -154,7 +157,8 @@ __device__ __forceinline__ u32 take_group(ExpandSmem &s, u32 lane) {
 // its position), with the next window's edge-target load in flight before
 // the current window's shared-memory atomics. Called by every thread of the
 // CTA; s.next_group must be zero.
-__device__ __forceinline__ void expand_unit(ExpandSmem &s, u32 *row, u32 *summ, const uint2 *__restrict__ rows,
+template <int NW>
+__device__ __forceinline__ void expand_unit(ExpandSmemT<NW> &s, u32 *row, u32 *summ, const uint2 *__restrict__ rows,
                                             const u32 *__restrict__ val, const Unit &U, u32 lane, u32 warp, u32 lt,
                                             u32 le) {
     u32 grp = take_group(s, lane);
@@ -444,13 +448,14 @@ bitmat_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val
 // every row x of a's out-edges instead of into row a. The base rule
 // sg(x, y) :- e(p, x), e(p, y), x != y is the same step on the units
 // (p, rows {p}) with bit x cleared from R when it is folded into row x.
+template <int NW>
 struct SgSmem {
-    ExpandSmem e;
+    ExpandSmemT<NW> e;
     Unit cur, next;
     u32 next_x;                      // next fold target of the unit (a's out-edge index)
     u32 nlist;                       // touched words of R in the list
-    u64 res[UW][4];                  // per warp: next-delta rows [cur, end), unit slots [cur, end)
-    unsigned long long acc[UW][3];   // per warp: new tuples, next-step bound, rows written
+    u64 res[NW][4];                  // per warp: next-delta rows [cur, end), unit slots [cur, end)
+    unsigned long long acc[NW][3];   // per warp: new tuples, next-step bound, rows written
     // followed by: u32 row[words], u32 summ[swords], u32 lk[words], u32 lv[words]
     // (the touched words of R as a list: index, value)
 };
@@ -473,14 +478,19 @@ __device__ __forceinline__ void sg_close_range(u64 *res, u32 x, u64 start, u64 l
     }
 }
 
-__global__ void __launch_bounds__(UT, 4)
+// NT threads per CTA: 512 for long rows; 128 (16 CTAs per SM) when rows are
+// short enough, so that the many small units of SG run in more, smaller CTAs
+// (a unit's barriers then hold 4 warps instead of 16).
+template <int NT>
+__global__ void __launch_bounds__(NT, 2048 / NT)
 sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const uint2 *__restrict__ rows,
                     const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
                     uint2 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap, u64 unit_rows,
                     const u32 *__restrict__ hasout, StepCounters *__restrict__ ctr, u32 *err, int base_rule) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SgSmem &s = *reinterpret_cast<SgSmem *>(smem_raw);
-    u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(SgSmem));
+    constexpr int NW = NT / 32;
+    SgSmem<NW> &s = *reinterpret_cast<SgSmem<NW> *>(smem_raw);
+    u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(SgSmem<NW>));
     const u32 swords = (words + 31) / 32;
     u32 *summ = row + words;
     u32 *lk = summ + swords;
@@ -489,7 +499,7 @@ sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, co
     const u32 lt = lanemask_lt();
     const u32 le = lane == 31 ? ~0u : (2u << lane) - 1;
     const u32 nchunks = (swords + SCHUNK - 1) / SCHUNK;
-    for (u32 k = tid; k < words + swords; k += UT) row[k] = 0;
+    for (u32 k = tid; k < words + swords; k += NT) row[k] = 0;
     if (lane == 0) {
         s.res[warp][0] = s.res[warp][1] = s.res[warp][2] = s.res[warp][3] = 0;
         s.acc[warp][0] = s.acc[warp][1] = s.acc[warp][2] = 0;
@@ -511,7 +521,7 @@ sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, co
         expand_unit(s.e, row, summ, rows, val, U, lane, warp, lt, le);
         __syncthreads();  // (2) R is complete
         // ---- the touched words of R as a list (index, value), any order ----
-        for (u32 sw = tid; sw < swords; sw += UT) {
+        for (u32 sw = tid; sw < swords; sw += NT) {
             u32 bits = summ[sw];
             if (!bits) continue;
             u32 at = atomicAdd(&s.nlist, (u32) __popc(bits));
@@ -616,7 +626,7 @@ sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, co
         }
         __syncthreads();  // (4) every fold target is done with R
         // ---- clear R and its summary (the list holds every touched word) ----
-        for (u32 i2 = tid; i2 < nlist; i2 += UT) {
+        for (u32 i2 = tid; i2 < nlist; i2 += NT) {
             const u32 k = lk[i2];
             row[k] = 0;
             summ[k >> 5] = 0;
@@ -869,7 +879,7 @@ u64 bitmat_bytes(u64 n) { return n * bitmat_stride(n) * 4; }
 bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, int copies) {
     if (opt.dedup != DL_DEDUP_AUTO && opt.dedup != DL_DEDUP_BITMAP) return false;
     // a row (TC), or a row and its touched-word list (SG), must fit in shared memory
-    if ((n + 31) / 32 * 4 * (copies == 1 ? 3 : 1) + sizeof(SgSmem) + 4096 > 227 * 1024) return false;
+    if ((n + 31) / 32 * 4 * (copies == 1 ? 3 : 1) + sizeof(SgSmem<UW>) + 4096 > 227 * 1024) return false;
     const u64 need = (u64) copies * bitmat_bytes(n);
     size_t free_b = 0, total_b = 0;
     DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -1036,7 +1046,8 @@ u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &o
     const u64 stride = bitmat_stride(n);
     const u64 unit_rows = std::max<u64>(1, ctx.tune.bitmap_unit_rows);
     const u64 words_used = (n + 31) / 32;
-    const size_t smem = sizeof(SgSmem) + (3 * words_used + (words_used + 31) / 32) * 4 + 16;
+    const size_t row_smem = (3 * words_used + (words_used + 31) / 32) * 4 + 16;
+    const size_t smem = sizeof(SgSmem<UW>) + row_smem;
     if (smem > 227 * 1024) throw Error(DL_ERR_OUT_OF_MEMORY, "bit-matrix rows of " + std::to_string(n) +
                                                               " nodes do not fit in shared memory");
     DevBuf &M = ws.bitmat[0];
@@ -1061,11 +1072,16 @@ u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &o
     u64 bound = ctx.host_scalars[0];
     const uint2 *rows = ws.jbuf[1].as<uint2>();
     u64 nunits = n, nrows = n;
-    auto kern = sg_unit_step_kernel;
-    DL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    int per_sm = 0;
-    DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, UT, smem));
-    const u64 resident = (u64) ctx.sm_count * std::max(per_sm, 1);
+    // 128-thread CTAs when 8 or more of them fit on an SM (short rows), else 512
+    const size_t smem_s = sizeof(SgSmem<4>) + row_smem;
+    int per_sm_s = 0, per_sm = 0;
+    DL_CUDA(cudaFuncSetAttribute(sg_unit_step_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_s));
+    DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_s, sg_unit_step_kernel<128>, 128, smem_s));
+    DL_CUDA(cudaFuncSetAttribute(sg_unit_step_kernel<UT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sg_unit_step_kernel<UT>, UT, smem));
+    const bool small = per_sm_s >= 8;
+    const int nt = small ? 128 : UT;
+    const u64 resident = (u64) ctx.sm_count * std::max(small ? per_sm_s : per_sm, 1);
     u64 nfull = 0;
     int slot = 0;
     for (int it = 0;; ++it) {  // it 0: the base rule (sg.cu:170-217); then sg.cu:244-390
@@ -1073,7 +1089,7 @@ u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &o
         u64 nnew = 0, next_units = 0, next_rows = 0, next_bound = 0;
         if (nunits && bound) {
             const unsigned grid = (unsigned) std::min<u64>(nunits, resident);
-            const u64 warps = (u64) grid * UW;
+            const u64 warps = (u64) grid * (nt / 32);
             // New rows < bound; a warp's reservations are at least 3/4 used
             // (a switch leaves less than one summary word's rows, <= 1024,
             // behind). The buffer is also capped by the device memory left; a
@@ -1092,12 +1108,18 @@ u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &o
             ctx.reserve(*ubuf_next, ucap * sizeof(Unit));
             DL_CUDA(cudaMemsetAsync(ctr, 0, sizeof(StepCounters), ctx.stream));
             pt.mark(PH_DEDUP);
-            DL_LAUNCH(ctx, K_BITMAP_EXPAND, 8.0 * nrows + 16.0 * nunits,
-                      kern<<<grid, UT, smem, ctx.stream>>>(g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m,
-                                                           stride, (u32) words_used, obuf.as<uint2>(), ocap,
-                                                           ubuf_next->as<Unit>(), ucap, unit_rows,
-                                                           ws.bit_hasout.as<u32>(), ctr, &ctx.ctrl->err,
-                                                           it == 0 ? 1 : 0));
+            if (small)
+                DL_LAUNCH(ctx, K_BITMAP_EXPAND, 8.0 * nrows + 16.0 * nunits,
+                          sg_unit_step_kernel<128><<<grid, 128, smem_s, ctx.stream>>>(
+                              g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m, stride, (u32) words_used,
+                              obuf.as<uint2>(), ocap, ubuf_next->as<Unit>(), ucap, unit_rows,
+                              ws.bit_hasout.as<u32>(), ctr, &ctx.ctrl->err, it == 0 ? 1 : 0));
+            else
+                DL_LAUNCH(ctx, K_BITMAP_EXPAND, 8.0 * nrows + 16.0 * nunits,
+                          sg_unit_step_kernel<UT><<<grid, UT, smem, ctx.stream>>>(
+                              g.csr.off, g.csr.val, rows, ubuf->as<Unit>(), nunits, m, stride, (u32) words_used,
+                              obuf.as<uint2>(), ocap, ubuf_next->as<Unit>(), ucap, unit_rows,
+                              ws.bit_hasout.as<u32>(), ctr, &ctx.ctrl->err, it == 0 ? 1 : 0));
             DL_CUDA(cudaMemcpyAsync(ctx.host_scalars, ctr, sizeof(StepCounters), cudaMemcpyDeviceToHost, ctx.stream));
             ctx.sync();  // a capacity overflow throws DL_ERR_OVERFLOW here
             next_rows = ctx.host_scalars[5];

@@ -11,7 +11,10 @@ released. Latency = completion time - arrival time.
 
 Admission is by an HBM budget: a request is admitted when the bytes the
 sessions hold plus the estimated peak bytes of the admitted, unfinished
-requests plus its own estimate stay within the budget. The estimate scales
+requests plus its own estimate stay within the budget. The budget is capped
+at construction by the device memory then free, less what each worker
+context may keep cached for reuse (`cache_gib`), so that the sessions'
+buffers always fit beside everything else on the device. The estimate scales
 with the input (rows x bytes-per-row per program); it is corrected upward
 whenever a finished request turns out larger than estimated. Requests are
 admitted in arrival order (no overtaking), and a request that does not fit
@@ -117,6 +120,15 @@ def percentiles(lat: list[float]) -> tuple[float, float, float, float]:
             float(a.max()))
 
 
+def device_headroom(device: int, workers: int, cache_gib: int, margin_gib: int = 2) -> int:
+    """Bytes the sessions may hold on `device`: the memory free now, less
+    `cache_gib` GiB of reuse cache per worker context and a margin for the
+    contexts' small fixed buffers."""
+    import torch
+    free, _ = torch.cuda.mem_get_info(device)
+    return max(0, int(free) - (workers * int(cache_gib) + margin_gib) * (1 << 30))
+
+
 class Server:
     """Continuous-batching server over one session per program.
 
@@ -147,13 +159,18 @@ class Server:
                     e = Engine(engine.device)
                     if tuning:
                         e.set_tuning(tuning)
-                    # buffers a worker keeps for reuse are outside the budget's
-                    # accounting: keep them small next to the other workers
+                    # buffers a worker keeps for reuse are outside the sessions'
+                    # accounting: keep them small and leave room for them below
                     e.set_tuning(cache_max_gib=cache_gib)
                     self._engines.append(e)
                     backend[p] = (lambda p=p, e=e: e.session(p, wcc_stop=wcc_stop))
             else:
                 backend = {p: (lambda p=p: engine.session(p, wcc_stop=wcc_stop)) for p in PROGRAMS}
+            if self._engines:
+                room = device_headroom(engine.device, len(self._engines), cache_gib)
+            else:  # the sessions share the caller's context and its cache limit
+                room = device_headroom(engine.device, 1, engine.tuning()["cache_max_gib"])
+            self.budget = min(self.budget, room)
         self._factory = backend
         self.sessions = {}
         self.row_bytes = dict(ROW_BYTES)

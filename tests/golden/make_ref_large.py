@@ -56,10 +56,13 @@ CASES = [
     # single_join's synthetic rows (glibc srand(1)/rand(), common/parallel_io.cu:79-108): the weak- and
     # strong-scaling inputs of one rank; the reference never writes this program's output file (job_run
     # is fixed at 1, single_join.cu:78), so these are pinned by counts
+    # (the log line before each cited result holds the command: rows, cuda_aware, comm_method, rand_range)
     ("single_join_weak", "single_join", "rows:10000000:500000", (199_915_594, 1),
-     "drawing/charts/single_join_weak (copy).csv:2"),
-    ("single_join_strong", "single_join", "rows:10000001:100000", (1_037_050_773, 1),
-     "drawing/charts/single_join_strong (copy).csv:2"),
+     "logs/single-join-small-job-output.txt:58"),
+    ("single_join_strong", "single_join", "rows:10000001:90000", (1_037_050_773, 1),
+     "logs/single-join-small-job-output.txt:106"),
+    ("single_join_10m_100k", "single_join", "rows:10000000:100000", (950_725_901, 1),
+     "logs/single-join-small-job-output.txt:10"),
 ]
 
 LARGE_FILES = sorted({c[2] for c in CASES if not c[2].startswith(("synthetic:", "rows:"))})
