@@ -318,6 +318,9 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
 
     stream = torch.cuda.Stream(device=dev)
     eng = Engine(local_rank, stream=stream)
+    knobs = {k: (float(v) if "." in v else int(v)) for k, v in (t.split("=", 1) for t in args.tuning)}
+    if knobs:
+        eng.set_tuning(knobs)
     d_edges = torch.from_numpy(edges).to(dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
 
@@ -388,6 +391,8 @@ def main_ours(args, rank: int, world: int, local_rank: int) -> int:
 
     if rank == 0:
         cfg = describe(args.config, edges)
+        if knobs:
+            cfg["tuning"] = knobs
         cfg.update({"parallelism": f"replicas x{world}", "l2": "256 MiB write between steps (outside timing)",
                     "output_tuples_per_step": int(r.output_tuples), "iterations": int(r.iterations),
                     "join_rows_per_step": int(r.join_rows_total), "join_rows_max_iteration": int(r.join_rows_max),
@@ -668,6 +673,8 @@ def main(argv=None) -> int:
                     help="skip the SG leg on the reference's fe_body input")
     ap.add_argument("--no-single-join-leg", dest="single_join_leg", action="store_false",
                     help="skip the single_join leg (10M rows, the reference's strong-scaling input)")
+    ap.add_argument("--tuning", action="append", default=[], metavar="KNOB=VALUE",
+                    help="engine knob for the main leg (dl_tuning field), e.g. bitmap_result=2; repeatable")
     ap.add_argument("--batch-instances", type=int, default=1024, help="batched form instances (0: skip)")
     ap.add_argument("--autotune", action="store_true",
                     help="re-run the autotuner for the batched leg instead of the committed knobs")

@@ -78,8 +78,9 @@ typedef enum dl_wcc_stop {
 
 /* How TC removes known tuples from a join output (same results either way). */
 typedef enum dl_dedup {
-    DL_DEDUP_AUTO = 0,  /* the engine's choice: BITMAP for TC when the bit matrix and its transpose
-                           fit in dl_tuning.bitmap_max_gib and half the free device memory, else SORT */
+    DL_DEDUP_AUTO = 0,  /* the engine's choice: BITMAP for TC when the bit matrix (and the column
+                           offsets of its result rows, 1/16 of its size) fit in
+                           dl_tuning.bitmap_max_gib and half the free device memory, else SORT */
     DL_DEDUP_SORT = 1,  /* radix sort of the join output + merge-path difference against sorted full */
     DL_DEDUP_HASH = 2,  /* full as a hash set of tuple words; one sort of the result at the end
                            (no per-iteration sort, but random-access bound: 1.7x slower on
@@ -142,10 +143,14 @@ typedef struct dl_tuning {
     int32_t sort_input_tma;       /* three-kernel pass input: 1 = TMA double buffer (default), 0 = direct loads */
     double hash_load_factor;      /* dl_build_hash_table's default load factor (0 < lf < 1, default 0.5) */
     int32_t join_first_pass;      /* TC: 1 = the join emit also does the sort's first radix pass (default), 0 = not */
-    int32_t bitmap_max_gib;       /* TC dedup AUTO: largest bit matrix + transpose, GiB (0..1024, default 48; 0 = never) */
+    int32_t bitmap_max_gib;       /* TC dedup AUTO: largest bit matrix + column offsets, GiB (0..1024, default 48; 0 = never) */
     int32_t bitmap_unit_rows;     /* bit-matrix TC: delta rows per work unit (1..16777216, default 65536) */
     int32_t cache_max_gib;        /* outgrown or released device buffers the context keeps for reuse, at most
                                      this many GiB (0..1024, default 96; 0 = free them at once) */
+    int32_t bitmap_result;        /* bit-matrix TC: how the result rows leave the matrix (same rows):
+                                     0 = through its transpose when a second matrix fits in bitmap_max_gib
+                                     and the free memory, else from its columns (default); 1 = transpose;
+                                     2 = columns (per 512-row block and target offsets, 1/16 of a matrix) */
 } dl_tuning;
 DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out);
 DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *tuning);

@@ -65,7 +65,8 @@ class dl_tuning(C.Structure):
     _fields_ = [("sort_algorithm", C.c_int32), ("sort_ranking", C.c_int32), ("sort_keys_per_thread", C.c_int32),
                 ("dense_ratio", C.c_int32), ("small_ratio", C.c_int32), ("sort_input_tma", C.c_int32),
                 ("hash_load_factor", C.c_double), ("join_first_pass", C.c_int32), ("bitmap_max_gib", C.c_int32),
-                ("bitmap_unit_rows", C.c_int32), ("cache_max_gib", C.c_int32)]
+                ("bitmap_unit_rows", C.c_int32), ("cache_max_gib", C.c_int32),
+                ("bitmap_result", C.c_int32)]
 
 
 class dl_kernel_stat(C.Structure):

@@ -8,9 +8,10 @@
 // full u J are one operation: a join tuple (x, w) is new exactly when its bit
 // goes from 0 to 1. The delta is the same set as the reference's (every new
 // bit is claimed by exactly one atomic on M), so per-iteration |delta| and the
-// fixpoint are identical. The result leaves as sorted (target, source) words
-// -- the reference's output order (tc.cu:345-366) -- through a bit-matrix
-// transpose, row popcounts, a scan and an extraction pass.
+// fixpoint are identical. The result rows leave in the reference's output
+// order (tc.cu:345-366: by target, then source) straight from M's columns:
+// a counting pass and a rows pass over M, each transposing 32 x 32 bit
+// blocks in registers.
 //
 // A delta is kept as units: one source x and a run of path targets y (u32,
 // at most `unit_rows` of them; Tuning::bitmap_unit_rows, default 65,536: a
@@ -30,8 +31,6 @@ namespace dl {
 namespace detail {
 namespace {
 
-constexpr int TR_ROWS = 512;  // source rows per transpose tile
-constexpr int TR_WORDS = 16;  // source words (512 columns) per transpose tile
 constexpr int UT = 512;       // threads of the unit kernel
 
 // One source x and delta rows rows[start, start + len): paths x -> y for
@@ -674,119 +673,9 @@ __global__ void bitmat_row_popc_kernel(const u32 *__restrict__ m, u64 n, u64 str
     }
 }
 
-// Lane l gets the word whose bit b is bit l of lane b's word (32 x 32 bit
-// transpose by recursive block swaps: each stage exchanges bit j of the row
-// index with bit j of the column index). The 16- and 8-bit stages move whole
-// bytes, so one byte permute does each.
-__device__ __forceinline__ u32 transpose32(u32 v, u32 lane) {
-    u32 u = __shfl_xor_sync(0xffffffffu, v, 16);
-    v = __byte_perm(v, u, (lane & 16) ? 0x3276 : 0x5410);
-    u = __shfl_xor_sync(0xffffffffu, v, 8);
-    v = __byte_perm(v, u, (lane & 8) ? 0x3715 : 0x6240);
-    const u32 masks[3] = {0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-        const int j = 4 >> s;
-        const u32 mk = masks[s];
-        u = __shfl_xor_sync(0xffffffffu, v, j);
-        v = (lane & j) ? ((v & ~mk) | ((u >> j) & mk)) : ((v & mk) | ((u & mk) << j));
-    }
-    return v;
-}
-
-__device__ __forceinline__ void cp_async4(u32 *dst, const u32 *src) {
-    const unsigned d = (unsigned) __cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
-// t = transpose of a (both n rows of `stride` words), and counts[w] += set
-// bits of target row w. A tile is 512 source rows x 512 columns: 64 bytes
-// read from every source row and 64 bytes written to every target row. CTA
-// (c, g) walks the tiles of column block c (targets 512 c ...) for source
-// blocks g, g + G, ...; the next tile is copied into shared memory (cp.async,
-// two buffers) while the current one is transposed and stored. Thread i keeps
-// the popcount of target row 512 c + i over its tiles and adds it to counts
-// once at the end (G atomics per row).
-constexpr int TR_PAD = TR_WORDS + 1;
-constexpr int TR_SMEM = 3 * TR_ROWS * TR_PAD * 4;  // two input tiles + the transposed tile
-__global__ void __launch_bounds__(TR_ROWS, 2) bitmat_transpose_count_kernel(const u32 *__restrict__ a,
-                                                                            u32 *__restrict__ t, u64 n, u64 stride,
-                                                                            unsigned long long *__restrict__ counts) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    u32(*in)[TR_ROWS][TR_PAD] = reinterpret_cast<u32(*)[TR_ROWS][TR_PAD]>(smem_raw);
-    u32(*outw)[TR_ROWS / 32 + 1] = reinterpret_cast<u32(*)[TR_ROWS / 32 + 1]>(smem_raw + 2 * TR_ROWS * TR_PAD * 4);
-    static_assert(TR_WORDS * 32 == TR_ROWS && TR_ROWS / 32 == TR_WORDS, "square tile: 512 x 512 bits");
-    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const u64 c0 = (u64) blockIdx.x * TR_WORDS;  // first column word of the block
-    const u64 nblocks = (n + TR_ROWS - 1) / TR_ROWS;
-    // A column block lies inside the row (stride is a multiple of 32 words);
-    // only the last block of source rows and of target rows can be partial.
-    const bool full_targets = c0 * 32 + TR_ROWS <= n;
-    const u32 r0 = tid / TR_WORDS, cc = tid % TR_WORDS;  // this thread's first (row, word) of a tile
-    auto issue = [&](u64 b, int buf) {  // tile (b, c) -> in[buf]
-        const u64 x0 = b * TR_ROWS;
-        const u32 *src = a + (x0 + r0) * stride + c0 + cc;
-        const u64 step = (u64) (TR_ROWS / TR_WORDS) * stride;  // 32 rows
-        if (x0 + TR_ROWS <= n) {
-#pragma unroll
-            for (u32 j = 0; j < TR_WORDS; ++j) cp_async4(&in[buf][r0 + 32 * j][cc], src + j * step);
-        } else {
-#pragma unroll
-            for (u32 j = 0; j < TR_WORDS; ++j) {
-                if (x0 + r0 + 32 * j < n) cp_async4(&in[buf][r0 + 32 * j][cc], src + j * step);
-                else in[buf][r0 + 32 * j][cc] = 0u;
-            }
-        }
-    };
-    u32 cnt = 0;  // set bits of target row c0 * 32 + tid in this CTA's tiles
-    u64 b = blockIdx.y;
-    int buf = 0;
-    if (b < nblocks) issue(b, 0);
-    cp_async_commit();
-    for (; b < nblocks; b += gridDim.y, buf ^= 1) {
-        // in[buf ^ 1] was last read by the previous tile's transpose, which
-        // every thread finished before the barrier ahead of its stores
-        if (b + gridDim.y < nblocks) issue(b + gridDim.y, buf ^ 1);
-        cp_async_commit();
-        cp_async_wait_prev();  // this thread's copies of tile b have landed
-        __syncthreads();       // everyone's have
-#pragma unroll 4
-        for (u32 c = 0; c < TR_WORDS; ++c)
-            outw[c * 32 + lane][warp] = transpose32(in[buf][warp * 32 + lane][c], lane);
-        __syncthreads();
-#pragma unroll
-        for (u32 xw = 0; xw < TR_ROWS / 32; ++xw) cnt += __popc(outw[tid][xw]);
-        const u64 x0 = b * TR_ROWS;
-        u32 *dst = t + (c0 * 32 + r0) * stride + x0 / 32 + cc;
-        const u64 step = (u64) (TR_ROWS / TR_WORDS) * stride;  // 32 target rows
-        if (full_targets) {
-#pragma unroll 4
-            for (u32 j = 0; j < TR_WORDS; ++j) dst[j * step] = outw[r0 + 32 * j][cc];
-        } else {
-#pragma unroll 4
-            for (u32 j = 0; j < TR_WORDS; ++j)
-                if (c0 * 32 + r0 + 32 * j < n) dst[j * step] = outw[r0 + 32 * j][cc];
-        }
-        // outw is rewritten only after the next iteration's first barrier
-    }
-    const u64 w = c0 * 32 + tid;
-    if (w < n && cnt) atomicAdd(counts + w, (unsigned long long) cnt);
-}
-
-// Row w of t -> result rows for its set bits x, ascending, from
-// out[first[w]] on: (ids[x], ids[w]) for TC's transpose (the reference's TC
-// file order (x, z) sorted by (z, x)), (ids[w], ids[x]) for SG's matrix (its
-// order (x, y) sorted by (x, y)). One warp per row; a lane takes 4 consecutive words per step (one
-// 16-byte load, the next one in flight); a step's rows are staged in shared
-// memory and leave with consecutive stores unless there are more than
-// EX_STAGE of them. (Result words are sparse -- C1 averages well under one
-// set bit per non-zero word -- so each lane walks its own words' bits.)
-constexpr int EX_THREADS = 256;
-constexpr int EX_STAGE = 256;
-// a result row as one little-endian 8-byte word: (column id, row id) for TC
-// (rows (x, z) of the transpose's row z), (row id, column id) for SG
+// a result row as one little-endian 8-byte word: (column id, row id) for a
+// matrix row's bits read as column ids (TC's (x, z) of target z), (row id,
+// column id) for SG's rows
 template <bool RowFirst>
 __device__ __forceinline__ u64 pack_row(u32 row_id, u32 col_id) {
     return RowFirst ? ((u64) col_id << 32) | row_id : ((u64) row_id << 32) | col_id;
@@ -794,9 +683,292 @@ __device__ __forceinline__ u64 pack_row(u32 row_id, u32 col_id) {
 __device__ __forceinline__ u32 xid(const int32_t *__restrict__ ids, bool affine, int32_t base, u64 x) {
     return (u32) (affine ? (int32_t) (base + (int64_t) x) : __ldg(ids + x));
 }
+
+// a[r] bit b -> a[b] bit r: a 32 x 32 bit transpose inside one thread's
+// registers by recursive block swaps (round j exchanges bit j of the row
+// index with bit j of the bit index; H. S. Warren, Hacker's Delight, 2nd
+// ed., section 7-3).
+__device__ __forceinline__ void transpose32_regs(u32 (&a)[32]) {
+    // rounds 16 and 8 move whole half-words and bytes: one byte permute per word
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const u32 lo = a[k], hi = a[k + 16];
+        a[k] = __byte_perm(lo, hi, 0x5410);
+        a[k + 16] = __byte_perm(lo, hi, 0x7632);
+    }
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        if (k & 8) continue;
+        const u32 lo = a[k], hi = a[k + 8];
+        a[k] = __byte_perm(lo, hi, 0x6240);
+        a[k + 8] = __byte_perm(lo, hi, 0x7351);
+    }
+#pragma unroll
+    for (int j = 4; j >= 1; j >>= 1) {
+        const u32 m = j == 4 ? 0x0F0F0F0Fu : j == 2 ? 0x33333333u : 0x55555555u;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            if (k & j) continue;
+            const u32 t = ((a[k] >> j) ^ a[k + j]) & m;
+            a[k + j] ^= t;
+            a[k] ^= t << j;
+        }
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    const unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// TC's result rows (x, z) in the reference's order (by z, then x) come from
+// the columns of the matrix M (row x, bit z). Two passes walk M in tiles of
+// CX_ROWS source rows x CX_WORDS column words (128 bytes of every row, read
+// with 16-byte cp.async into shared memory, the next tile in flight while
+// the current one is worked on):
+//   count pass: per tile and target z, the set bits of column z in the
+//     tile's rows -> off[xb][z] (xb = the tile's row block);
+//   a column scan turns off[.][z] into offsets within column z, a scan of
+//     the column totals gives each z its first row;
+//   rows pass: the same walk writes every set bit (x, z) of a tile to
+//     out[first[z] + off[xb][z] + rank of x among the tile's bits of z].
+// In a tile, thread (warp w, lane l) reads the 32 x 32 bit block (row block
+// rb = l % 16, column word cw = (w + l) % 32) one row at a time -- the 32
+// lanes read 32 different column words, so no bank conflicts -- transposes
+// it in registers and stores the 32 target words to a target-major tile
+// (1024 targets x 16 words); four lanes then take each target row, 4 words
+// (one 16-byte load) each.
+constexpr int CX_ROWS = 512;                  // source rows of a tile
+constexpr int CX_WORDS = 32;                  // column words of a tile
+constexpr int CX_TARGETS = CX_WORDS * 32;     // targets of a tile
+constexpr int CX_XW = CX_ROWS / 32;           // words of a target row in a tile
+constexpr int CX_THREADS = 512;
+struct ColSmem {
+    u32 in[2][CX_ROWS][CX_WORDS];  // source tiles (two buffers)
+    u32 outw[CX_TARGETS][CX_XW];   // the current tile, target-major
+    u64 base[CX_TARGETS];          // rows pass: first output row of each target in this tile
+    u32 cnt[CX_TARGETS];           // count pass: set bits of each target in this tile
+};
+static_assert(CX_WORDS == 32 && CX_ROWS / 32 == CX_THREADS / 32, "one block per thread and tile");
+
+enum ColMode { COL_COUNT = 0, COL_ROWS = 1, COL_TRANSPOSE = 2 };
+
+template <int MODE>
+__device__ __forceinline__ void bitmat_columns_body(const u32 *__restrict__ m, u64 n, u64 stride, u64 xblocks,
+                                                    u64 t_first, u64 tiles, u32 *__restrict__ off,
+                                                    const u64 *__restrict__ first,
+                                                    const int32_t *__restrict__ ids, bool affine, int32_t base,
+                                                    u64 *__restrict__ out, u32 *__restrict__ tout,
+                                                    unsigned long long *__restrict__ counts) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ColSmem &s = *reinterpret_cast<ColSmem *>(smem_raw);
+    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // tiles are numbered column block major; CTA k takes a contiguous range
+    // of tiles [t_first, t_first + tiles)
+    const u64 t_begin = t_first + tiles * blockIdx.x / gridDim.x;
+    const u64 t_end = t_first + tiles * (blockIdx.x + 1) / gridDim.x;
+    auto issue = [&](u64 t, int buf) {  // 16-byte chunks tid, tid + 512, ...: 8 per source row
+        const u64 x0 = (t % xblocks) * CX_ROWS;
+        const u32 *src = m + (t / xblocks) * CX_WORDS;
+#pragma unroll
+        for (int i = 0; i < CX_ROWS * CX_WORDS / 4 / CX_THREADS; ++i) {
+            const u32 chunk = tid + i * CX_THREADS;
+            const u32 r = chunk / (CX_WORDS / 4), c4 = chunk % (CX_WORDS / 4);
+            u32 *dst = &s.in[buf][r][c4 * 4];
+            if (x0 + r < n) cp_async16(dst, src + (x0 + r) * stride + c4 * 4);
+            else *reinterpret_cast<uint4 *>(dst) = make_uint4(0u, 0u, 0u, 0u);
+        }
+    };
+    const u32 rb = lane & 15, cw = (warp + lane) & 31, hi = lane >> 4;
+    const u32 q = tid & 3;  // this thread's quarter of a target row
+    constexpr int TPT = CX_TARGETS * 4 / CX_THREADS;  // target quarters per thread and tile
+    if constexpr (MODE == COL_COUNT) {
+        for (u32 i = tid; i < CX_TARGETS; i += CX_THREADS) s.cnt[i] = 0;  // ordered by barrier (1)
+    }
+    // transpose: set bits of this thread's target quarters in the current column block
+    u32 tcnt[TPT];
+#pragma unroll
+    for (int k = 0; k < TPT; ++k) tcnt[k] = 0;
+    u64 tcb = t_begin < t_end ? t_begin / xblocks : 0;
+    auto flush_counts = [&](u64 cb) {  // the four quarters of a target are lanes 4j..4j+3
+#pragma unroll
+        for (int k = 0; k < TPT; ++k) {
+            u32 c = tcnt[k];
+            c += __shfl_xor_sync(0xffffffffu, c, 1);
+            c += __shfl_xor_sync(0xffffffffu, c, 2);
+            const u64 z = cb * CX_TARGETS + (tid >> 2) + k * (CX_THREADS / 4);
+            if (q == 0 && c && z < n) atomicAdd(counts + z, (unsigned long long) c);
+            tcnt[k] = 0;
+        }
+    };
+    int buf = 0;
+    if (t_begin < t_end) issue(t_begin, 0);
+    cp_async_commit();
+    for (u64 t = t_begin; t < t_end; ++t, buf ^= 1) {
+        // s.in[buf ^ 1] was last read before the previous tile's second barrier
+        if (t + 1 < t_end) issue(t + 1, buf ^ 1);
+        cp_async_commit();
+        const u64 xb = t % xblocks, cb = t / xblocks, z0 = cb * CX_TARGETS;
+        u64 pb[CX_TARGETS / CX_THREADS];  // rows pass: first rows of targets tid, tid + 512 in this tile
+        if constexpr (MODE == COL_ROWS) {
+#pragma unroll
+            for (int k = 0; k < CX_TARGETS / CX_THREADS; ++k) {
+                const u64 z = z0 + tid + k * CX_THREADS;
+                pb[k] = z < n ? first[z] + off[xb * n + z] : 0;
+            }
+        }
+        if constexpr (MODE == COL_TRANSPOSE) {
+            if (cb != tcb) {  // uniform across the CTA
+                flush_counts(tcb);
+                tcb = cb;
+            }
+        }
+        cp_async_wait_prev();
+        __syncthreads();  // (1) tile t has landed; the previous tile's results are out
+        u32 a[32];
+        if constexpr (MODE == COL_COUNT) {
+            // counts only: rotate row words right by `lane` before the
+            // transpose, so that a[b] then belongs to target 32 cw + (b + lane)
+            // % 32 and the 32 lanes' shared-memory atomics hit 32 banks
+#pragma unroll
+            for (int r = 0; r < 32; ++r) {
+                const u32 w = s.in[buf][32 * rb + r][cw];
+                a[r] = __funnelshift_r(w, w, lane);
+            }
+            transpose32_regs(a);
+#pragma unroll
+            for (int b = 0; b < 32; ++b) {
+                const u32 c = __popc(a[b]);
+                if (c) atomicAdd(&s.cnt[32 * cw + ((b + lane) & 31)], c);
+            }
+            __syncthreads();  // (2) the tile's counts are complete
+            for (u32 i = tid; i < CX_TARGETS; i += CX_THREADS) {
+                const u64 z = z0 + i;
+                if (z < n) off[xb * n + z] = s.cnt[i];
+                s.cnt[i] = 0;
+            }
+        } else {
+            if constexpr (MODE == COL_ROWS) {
+#pragma unroll
+                for (int k = 0; k < CX_TARGETS / CX_THREADS; ++k) s.base[tid + k * CX_THREADS] = pb[k];
+            }
+#pragma unroll
+            for (int r = 0; r < 32; ++r) a[r] = s.in[buf][32 * rb + r][cw];
+            transpose32_regs(a);
+            // a[b] = word rb of target 32 cw + b; the upper half-warp stores
+            // b ^ 1 while the lower stores b, so the 32 stores hit 32 banks
+#pragma unroll
+            for (int b = 0; b < 32; ++b) s.outw[32 * cw + (b ^ hi)][rb] = hi ? a[b ^ 1] : a[b];
+            __syncthreads();  // (2) the target-major tile is complete
+            if constexpr (MODE == COL_TRANSPOSE) {
+                // four lanes per target row segment (64 bytes): 8 targets per warp store
+#pragma unroll
+                for (int k = 0; k < TPT; ++k) {
+                    const u32 i = (tid >> 2) + k * (CX_THREADS / 4);
+                    const uint4 w4 = *reinterpret_cast<const uint4 *>(&s.outw[i][4 * q]);
+                    tcnt[k] += __popc(w4.x) + __popc(w4.y) + __popc(w4.z) + __popc(w4.w);
+                    const u64 z = z0 + i;
+                    if (z < n) *reinterpret_cast<uint4 *>(tout + z * stride + xb * CX_XW + 4 * q) = w4;
+                }
+            } else {
+                // four lanes per target, four words (128 source rows) per lane
+#pragma unroll 2
+                for (u32 i = tid >> 2; i < CX_TARGETS; i += CX_THREADS / 4) {
+                    const uint4 w4 = *reinterpret_cast<const uint4 *>(&s.outw[i][4 * q]);
+                    const u32 c = __popc(w4.x) + __popc(w4.y) + __popc(w4.z) + __popc(w4.w);
+                    u32 incl = c;
+                    u32 y = __shfl_up_sync(0xffffffffu, incl, 1, 4);
+                    if (q >= 1) incl += y;
+                    y = __shfl_up_sync(0xffffffffu, incl, 2, 4);
+                    if (q >= 2) incl += y;
+                    const u64 z = z0 + i;
+                    if (z >= n || c == 0) continue;
+                    u64 p = s.base[i] + (incl - c);
+                    const u32 zid = xid(ids, affine, base, z);
+                    const u64 x0 = (xb * CX_XW + 4 * q) * 32;
+                    // the lane's 128 bits as one sequence: one pass per set bit
+                    u64 lo = ((u64) w4.y << 32) | w4.x, hi2 = ((u64) w4.w << 32) | w4.z;
+                    while (lo | hi2) {
+                        u32 bit;
+                        if (lo) {
+                            bit = (u32) __ffsll((long long) lo) - 1;
+                            lo &= lo - 1;
+                        } else {
+                            bit = 64 + (u32) __ffsll((long long) hi2) - 1;
+                            hi2 &= hi2 - 1;
+                        }
+                        out[p++] = pack_row<false>(zid, xid(ids, affine, base, x0 + bit));
+                    }
+                }
+            }
+        }
+    }
+    if constexpr (MODE == COL_TRANSPOSE) {
+        if (t_begin < t_end) flush_counts(tcb);
+    }
+}
+
+__global__ void __launch_bounds__(CX_THREADS, 1)
+bitmat_column_count_kernel(const u32 *__restrict__ m, u64 n, u64 stride, u64 xblocks, u64 tiles,
+                           u32 *__restrict__ off) {
+    bitmat_columns_body<COL_COUNT>(m, n, stride, xblocks, 0, tiles, off, nullptr, nullptr, false, 0, nullptr,
+                                   nullptr, nullptr);
+}
+
+__global__ void __launch_bounds__(CX_THREADS, 1)
+bitmat_column_rows_kernel(const u32 *__restrict__ m, u64 n, u64 stride, u64 xblocks, u64 t_first, u64 tiles,
+                          const u32 *__restrict__ off, const u64 *__restrict__ first,
+                          const int32_t *__restrict__ ids, bool affine, int32_t base, u64 *__restrict__ out) {
+    bitmat_columns_body<COL_ROWS>(m, n, stride, xblocks, t_first, tiles, const_cast<u32 *>(off), first, ids, affine,
+                                  base, out, nullptr, nullptr);
+}
+
+// t = the transpose of m (n rows of `stride` words each), counts[z] += the
+// set bits of row z of t (counts zeroed by the caller).
+__global__ void __launch_bounds__(CX_THREADS, 1)
+bitmat_transpose_count_kernel(const u32 *__restrict__ m, u64 n, u64 stride, u64 xblocks, u64 tiles,
+                              u32 *__restrict__ t, unsigned long long *__restrict__ counts) {
+    bitmat_columns_body<COL_TRANSPOSE>(m, n, stride, xblocks, 0, tiles, nullptr, nullptr, nullptr, false, 0, nullptr,
+                                       t, counts);
+}
+
+// off[.][z]: per row block counts of column z -> exclusive prefix over the
+// row blocks; tot[z] = the column's total (at most n < 2^31 bits).
+__global__ void column_offsets_kernel(u32 *__restrict__ off, u64 n, u64 xblocks, unsigned long long *__restrict__ tot) {
+    const u64 z = (u64) blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= n) return;
+    u32 run = 0;
+    u64 xb = 0;
+    for (; xb + 4 <= xblocks; xb += 4) {
+        u32 *p = off + xb * n + z;
+        const u32 c0 = p[0], c1 = p[n], c2 = p[2 * n], c3 = p[3 * n];
+        p[0] = run;
+        p[n] = run += c0;
+        p[2 * n] = run += c1;
+        p[3 * n] = run += c2;
+        run += c3;
+    }
+    for (; xb < xblocks; ++xb) {
+        const u32 c = off[xb * n + z];
+        off[xb * n + z] = run;
+        run += c;
+    }
+    tot[z] = run;
+}
+
+// Row w of the matrix -> result rows (ids[w], ids[x]) for its set bits x,
+// ascending, from out[first[w]] on (SG's order: (x, y) sorted by (x, y)).
+// One warp per row; a lane takes 4 consecutive words per step (one 16-byte
+// load, the next one in flight); a step's rows are staged in shared memory
+// and leave with consecutive stores unless there are more than EX_STAGE of
+// them. (Result words are sparse, so each lane walks its own words' bits.)
+constexpr int EX_THREADS = 256;
+constexpr int EX_STAGE = 256;
 template <bool RowFirst>
-__global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u32 *__restrict__ t, u64 n,
-                                                                         u64 stride, u64 words,
+__global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u32 *__restrict__ t, u64 w_begin,
+                                                                         u64 w_end, u64 stride, u64 words,
                                                                          const u64 *__restrict__ first,
                                                                          const int32_t *__restrict__ ids,
                                                                          bool affine, int32_t base,
@@ -805,7 +977,7 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     u64 *st = stage[warp];
     const u64 warps = (u64) gridDim.x * (EX_THREADS / 32);
-    for (u64 w = (u64) blockIdx.x * (EX_THREADS / 32) + warp; w < n; w += warps) {
+    for (u64 w = w_begin + (u64) blockIdx.x * (EX_THREADS / 32) + warp; w < w_end; w += warps) {
         const u32 *row = t + w * stride;
         u64 pos = first[w];
         // a dense id range needs no table lookup (ids[r] == base + r)
@@ -875,12 +1047,14 @@ u64 exclusive_scan(Context &ctx, const u64 *in, u64 n, u64 *out) {
 
 u64 bitmat_stride(u64 n) { return ((n + 31) / 32 + 31) / 32 * 32; }
 u64 bitmat_bytes(u64 n) { return n * bitmat_stride(n) * 4; }
+u64 bitmat_column_offset_bytes(u64 n) { return std::max<u64>((n + CX_ROWS - 1) / CX_ROWS * n * 4, 4); }
 
-bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, int copies) {
+bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, bool sg) {
     if (opt.dedup != DL_DEDUP_AUTO && opt.dedup != DL_DEDUP_BITMAP) return false;
     // a row (TC), or a row and its touched-word list (SG), must fit in shared memory
-    if ((n + 31) / 32 * 4 * (copies == 1 ? 3 : 1) + sizeof(SgSmem<UW>) + 4096 > 227 * 1024) return false;
-    const u64 need = (u64) copies * bitmat_bytes(n);
+    if ((n + 31) / 32 * 4 * (sg ? 3 : 1) + sizeof(SgSmem<UW>) + 4096 > 227 * 1024) return false;
+    // TC also keeps the per (row block, target) offsets of its result rows
+    const u64 need = bitmat_bytes(n) + (sg ? 0 : bitmat_column_offset_bytes(n));
     size_t free_b = 0, total_b = 0;
     DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const u64 held = ctx.ws.bitmat[0].cap + ctx.ws.bitmat[1].cap;
@@ -895,6 +1069,20 @@ bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, int copies) {
     return need <= ((u64) ctx.tune.bitmap_max_gib << 30) && need <= avail / 2;
 }
 
+
+// Whether a TC run's result rows leave through the matrix's transpose (a
+// second n x n matrix; the faster form) rather than from its columns.
+static bool tc_result_by_transpose(Context &ctx, u64 n) {
+    if (ctx.tune.bitmap_result == 1) return true;
+    if (ctx.tune.bitmap_result == 2) return false;
+    const u64 need = bitmat_bytes(n);
+    if (2 * need > ((u64) ctx.tune.bitmap_max_gib << 30)) return false;
+    size_t free_b = 0, total_b = 0;
+    DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    u64 cached = ctx.ws.bitmat[1].cap;
+    for (const DevBuf &b : ctx.spares) cached += b.cap;
+    return need + (1ull << 30) <= (u64) free_b + cached;
+}
 
 u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u64 ne, const dl_options &opt,
                        PhaseTimer &pt) {
@@ -1002,34 +1190,54 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         if (opt.max_iterations > 0 && it + 1 >= opt.max_iterations) break;
     }
     pt.mark(PH_FINAL);
-    // full -> its transpose (row = target) and per-target counts; the result
-    // rows are extracted from it when they are copied out (bitmat_extract_rows)
+    // The result rows are written when they are copied out
+    // (bitmat_extract_rows), in the reference's order (by target, then
+    // source), from either
+    //  - the transpose T of M (row = target) and each target's first row,
+    //    when a second matrix fits (bitmap_result 0 or 1), or
+    //  - M's columns, with per (512-row block, target) offsets (1/16 of a
+    //    matrix) and each target's first row (bitmap_result 2, or 0 when the
+    //    transpose does not fit).
     if (nfull) {
-        DevBuf &T = ws.bitmat[1];
-        ctx.reserve(T, bitmat_bytes(n));
+        const u64 xblocks = (n + CX_ROWS - 1) / CX_ROWS, tiles = (stride / CX_WORDS) * xblocks;
+        const unsigned cg = (unsigned) std::min<u64>(tiles, (u64) ctx.sm_count);
         ctx.reserve(ws.offsets, (n + 1) * 8);
         u64 *counts = ws.offsets.as<u64>();
-        DL_CUDA(cudaMemsetAsync(counts, 0, n * 8, ctx.stream));
-        DL_CUDA(cudaFuncSetAttribute(bitmat_transpose_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     TR_SMEM));
-        int tr_per_sm = 0;
-        DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tr_per_sm, bitmat_transpose_count_kernel, TR_ROWS,
-                                                              TR_SMEM));
-        const u64 xblocks = stride / TR_WORDS, nblocks = (n + TR_ROWS - 1) / TR_ROWS;
-        const u64 resident_tr = (u64) ctx.sm_count * std::max(tr_per_sm, 1);
-        const u64 gy = std::min<u64>(nblocks, std::max<u64>(1, (8 * resident_tr + xblocks - 1) / xblocks));
-        const dim3 tg((unsigned) xblocks, (unsigned) gy);
-        DL_LAUNCH(ctx, K_BITMAP_TRANSPOSE, 2.0 * bitmat_bytes(n),
-                  bitmat_transpose_count_kernel<<<tg, TR_ROWS, TR_SMEM, ctx.stream>>>(
-                      m, T.as<u32>(), n, stride, reinterpret_cast<unsigned long long *>(counts)));
+        const bool by_transpose = tc_result_by_transpose(ctx, n);
+        DevBuf &O = ws.bitmat[1];  // T, or the column offsets
+        if (by_transpose) {
+            ctx.reserve(O, bitmat_bytes(n));
+            DL_CUDA(cudaMemsetAsync(counts, 0, n * 8, ctx.stream));
+            DL_CUDA(cudaFuncSetAttribute(bitmat_transpose_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int) sizeof(ColSmem)));
+            DL_LAUNCH(ctx, K_BITMAP_COLUMNS, 2.0 * bitmat_bytes(n),
+                      bitmat_transpose_count_kernel<<<cg, CX_THREADS, sizeof(ColSmem), ctx.stream>>>(
+                          m, n, stride, xblocks, tiles, O.as<u32>(), reinterpret_cast<unsigned long long *>(counts)));
+        } else {
+            ctx.reserve(O, bitmat_column_offset_bytes(n));
+            DL_CUDA(cudaFuncSetAttribute(bitmat_column_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int) sizeof(ColSmem)));
+            DL_LAUNCH(ctx, K_BITMAP_COLUMNS, 1.0 * bitmat_bytes(n) + 4.0 * xblocks * n,
+                      bitmat_column_count_kernel<<<cg, CX_THREADS, sizeof(ColSmem), ctx.stream>>>(
+                          m, n, stride, xblocks, tiles, O.as<u32>()));
+            DL_LAUNCH(ctx, K_BITMAP_COLUMNS, 8.0 * xblocks * n + 8.0 * n,
+                      column_offsets_kernel<<<grid_for(n, T256, ctx, 64), T256, 0, ctx.stream>>>(
+                          O.as<u32>(), n, xblocks, reinterpret_cast<unsigned long long *>(counts)));
+        }
         ctx.reserve(ws.w0, (n + 1) * 8);
-        u64 *first = ws.w0.as<u64>();
-        const u64 total = exclusive_scan(ctx, counts, n, first);
+        const u64 total = exclusive_scan(ctx, counts, n, ws.w0.as<u64>());
         if (total != nfull)
             throw Error(DL_ERR_INTERNAL, "bit matrix holds " + std::to_string(total) + " tuples, expected " +
                                              std::to_string(nfull));
-        r.bm_t = T;
-        T = DevBuf();
+        if (by_transpose) {
+            r.bm_t = O;  // M stays in the workspace for the next run
+        } else {
+            r.bm_t = M;
+            M = DevBuf();
+            r.bm_off = O;
+            r.bm_cols = true;
+        }
+        O = DevBuf();
         r.bm_first = ws.w0;
         ws.w0 = DevBuf();
         r.bm_n = n;
@@ -1178,28 +1386,56 @@ u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &o
 static unsigned extract_grid(Context &ctx, u64 n) {
     using namespace detail;
     int per_sm = 0;
-    DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bitmat_extract_rows_kernel<false>, EX_THREADS, 0));
+    DL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bitmat_extract_rows_kernel<true>, EX_THREADS, 0));
     const u64 wave = (u64) ctx.sm_count * std::max(per_sm, 1);
     return (unsigned) std::max<u64>(1, std::min<u64>(wave, (n + EX_THREADS / 32 - 1) / (EX_THREADS / 32)));
 }
 
-// The result rows of a bit-matrix TC run, written straight from the stored
-// transpose into `out` (device memory): (x, z) rows ordered by (z, x).
-void bitmat_extract_rows(Context &ctx, const Run &r, int32_t *out) {
+// The result rows of a bit-matrix run leave in units: TC's column blocks
+// (1024 targets: rows (x, z) ordered by (z, x), from the matrix's columns)
+// or SG's matrix rows (rows (x, y) ordered by (x, y)).
+u64 bitmat_units(const Run &r) {
     using namespace detail;
-    if (r.info.output_rows == 0) return;
+    return r.bm_cols ? r.bm_stride / CX_WORDS : r.bm_n;
+}
+
+// Index into bm_first of the first target (TC) or row (SG) of `unit`; n for
+// the end.
+u64 bitmat_unit_index(const Run &r, u64 unit) {
+    using namespace detail;
+    return std::min<u64>(r.bm_n, r.bm_cols ? unit * CX_TARGETS : unit);
+}
+
+// The rows of units [u0, u1) into their places in `out` (device memory, all
+// result rows). Units are the rows of the stored matrix (SG's M, TC's
+// transpose) or, for TC from M's columns, its column blocks.
+void bitmat_extract_rows(Context &ctx, const Run &r, int32_t *out, u64 u0, u64 u1) {
+    using namespace detail;
+    if (r.info.output_rows == 0 || u0 >= u1) return;
     const u64 n = r.bm_n;
-    const double bytes = 4.0 * n * r.bm_words + 8.0 * (double) r.info.output_rows;
-    if (r.bm_row_first)
-        DL_LAUNCH(ctx, K_BITMAP_EXTRACT, bytes,
-                  bitmat_extract_rows_kernel<true><<<extract_grid(ctx, n), EX_THREADS, 0, ctx.stream>>>(
-                      r.bm_t.as<u32>(), n, r.bm_stride, r.bm_words, r.bm_first.as<u64>(), r.ids.as<int32_t>(),
-                      r.ids_affine, r.id_base, reinterpret_cast<u64 *>(out)));
-    else
-        DL_LAUNCH(ctx, K_BITMAP_EXTRACT, bytes,
-                  bitmat_extract_rows_kernel<false><<<extract_grid(ctx, n), EX_THREADS, 0, ctx.stream>>>(
-                      r.bm_t.as<u32>(), n, r.bm_stride, r.bm_words, r.bm_first.as<u64>(), r.ids.as<int32_t>(),
-                      r.ids_affine, r.id_base, reinterpret_cast<u64 *>(out)));
+    if (!r.bm_cols) {
+        if (r.bm_row_first)
+            DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 4.0 * (u1 - u0) * r.bm_words,
+                      bitmat_extract_rows_kernel<true><<<extract_grid(ctx, u1 - u0), EX_THREADS, 0, ctx.stream>>>(
+                          r.bm_t.as<u32>(), u0, u1, r.bm_stride, r.bm_words, r.bm_first.as<u64>(),
+                          r.ids.as<int32_t>(), r.ids_affine, r.id_base, reinterpret_cast<u64 *>(out)));
+        else
+            DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 4.0 * (u1 - u0) * r.bm_words,
+                      bitmat_extract_rows_kernel<false><<<extract_grid(ctx, u1 - u0), EX_THREADS, 0, ctx.stream>>>(
+                          r.bm_t.as<u32>(), u0, u1, r.bm_stride, r.bm_words, r.bm_first.as<u64>(),
+                          r.ids.as<int32_t>(), r.ids_affine, r.id_base, reinterpret_cast<u64 *>(out)));
+        return;
+    }
+    const u64 xblocks = (n + CX_ROWS - 1) / CX_ROWS, tiles = (u1 - u0) * xblocks;
+    DL_CUDA(cudaFuncSetAttribute(bitmat_column_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int) sizeof(ColSmem)));
+    const unsigned cg = (unsigned) std::min<u64>(tiles, (u64) ctx.sm_count);
+    // algorithmic bytes: the units' columns of the matrix and their offsets
+    // (the rows' 8 bytes each are added by the caller)
+    DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 128.0 * xblocks * CX_ROWS * (u1 - u0) + 4.0 * xblocks * CX_TARGETS * (u1 - u0),
+              bitmat_column_rows_kernel<<<cg, CX_THREADS, sizeof(ColSmem), ctx.stream>>>(
+                  r.bm_t.as<u32>(), n, r.bm_stride, xblocks, u0 * xblocks, tiles, r.bm_off.as<u32>(),
+                  r.bm_first.as<u64>(), r.ids.as<int32_t>(), r.ids_affine, r.id_base, reinterpret_cast<u64 *>(out)));
 }
 
 }  // namespace dl

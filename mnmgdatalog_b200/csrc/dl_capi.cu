@@ -637,6 +637,7 @@ DL_API dl_status dl_context_get_tuning(const dl_context *ctx, dl_tuning *out) {
     out->bitmap_max_gib = t.bitmap_max_gib;
     out->bitmap_unit_rows = (int32_t) t.bitmap_unit_rows;
     out->cache_max_gib = t.cache_max_gib;
+    out->bitmap_result = t.bitmap_result;
     return DL_OK;
 }
 
@@ -653,6 +654,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     DL_REQUIRE(t->bitmap_max_gib >= 0 && t->bitmap_max_gib <= 1024, "bitmap_max_gib must be in 0..1024");
     DL_REQUIRE(t->bitmap_unit_rows >= 1 && t->bitmap_unit_rows <= (1 << 24), "bitmap_unit_rows must be in 1..16777216");
     DL_REQUIRE(t->cache_max_gib >= 0 && t->cache_max_gib <= 1024, "cache_max_gib must be in 0..1024");
+    DL_REQUIRE(t->bitmap_result >= 0 && t->bitmap_result <= 2, "bitmap_result must be 0, 1 or 2");
     dl::Tuning &o = ctx->c.tune;
     o.sort_algo = t->sort_algorithm;
     o.rank = t->sort_ranking;
@@ -665,6 +667,7 @@ DL_API dl_status dl_context_set_tuning(dl_context *ctx, const dl_tuning *t) {
     o.bitmap_max_gib = t->bitmap_max_gib;
     o.bitmap_unit_rows = (uint32_t) t->bitmap_unit_rows;
     o.cache_max_gib = t->cache_max_gib;
+    o.bitmap_result = t->bitmap_result;
     ctx->c.trim_spares();
     return DL_OK;
 }

@@ -120,10 +120,20 @@ void Context::give_back(DevBuf &buf) {
     trim_spares();
 }
 
+cudaStream_t Context::copy_stream_get() {
+    if (!copy_stream) DL_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    return copy_stream;
+}
+
 void Context::release_all() {
     prof_resolve();
     for (auto e : ev_pool) cudaEventDestroy(e);
     ev_pool.clear();
+    if (copy_stream) {
+        cudaStreamSynchronize(copy_stream);
+        cudaStreamDestroy(copy_stream);
+        copy_stream = nullptr;
+    }
     for (auto &s : spares) s.release();
     spares.clear();
     DevBuf *all[] = {&ws.input, &ws.ids, &ws.w0, &ws.w1, &ws.csr_off, &ws.csr_val, &ws.full[0], &ws.full[1],
@@ -172,7 +182,7 @@ const char *kernel_name(int kid) {
     static const char *names[K_COUNT] = {"prep", "sort_histogram", "sort_spine_scan", "sort_scatter_pass",
                                          "select_compact", "join_count_scan", "join_partition", "join_emit",
                                          "wcc_propagate", "merge_partition", "diff_merge", "merge", "hash_build",
-                                         "sparse_diff", "hash_insert", "bitmap_expand", "bitmap_transpose", "bitmap_extract", "host_cudaMalloc", "host_cudaFree",
+                                         "sparse_diff", "hash_insert", "bitmap_expand", "bitmap_columns", "bitmap_extract", "host_cudaMalloc", "host_cudaFree",
                                          "host_sync"};
     return (kid >= 0 && kid < K_COUNT) ? names[kid] : "?";
 }

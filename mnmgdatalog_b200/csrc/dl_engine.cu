@@ -491,7 +491,7 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         // result rows then need no rank -> id table lookups.
         const bool dense = densify_ids(ctx, g, [&](u64 range) {
             try {
-                return bitmat_choose(ctx, opt, range, 2);
+                return bitmat_choose(ctx, opt, range, false);
             } catch (const Error &) {  // a forced bit matrix that fits only without the absent ids
                 return false;
             }
@@ -503,8 +503,8 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         u64 ne;
         u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, n, 2 * g.bits, ne);
         build_csr(ctx, e, ne, g);
-        if (dense || bitmat_choose(ctx, opt, g.n_ids, 2)) {
-            nfull = tc_bitmap_fixpoint(ctx, r, g, e, ne, opt, pt);  // result: the transpose, in r
+        if (dense || bitmat_choose(ctx, opt, g.n_ids, false)) {
+            nfull = tc_bitmap_fixpoint(ctx, r, g, e, ne, opt, pt);  // result: the matrix and its column offsets, in r
             cur = 0;
         } else {
             u64 nd;
@@ -646,7 +646,7 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         // As for TC: a dense id range is ranked as is when the bit matrix is used.
         const bool dense = densify_ids(ctx, g, [&](u64 range) {
             try {
-                return bitmat_choose(ctx, opt, range, 1);
+                return bitmat_choose(ctx, opt, range, true);
             } catch (const Error &) {
                 return false;
             }
@@ -654,7 +654,7 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         u64 ne;
         u64 *e = sg_edge_words(ctx, rows, n, g, ne);  // sg.cu:150-153
         build_csr(ctx, e, ne, g);                     // sg.cu:162
-        if (dense || bitmat_choose(ctx, opt, g.n_ids, 1)) {
+        if (dense || bitmat_choose(ctx, opt, g.n_ids, true)) {
             try {
                 nfull = sg_bitmap_fixpoint(ctx, r, g, opt, pt);
                 on_bitmat = true;
@@ -668,6 +668,7 @@ static void run_sg_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
                 r.from_bitmat = false;
                 ctx.give_back(r.bm_t);
                 ctx.give_back(r.bm_first);
+                ctx.give_back(r.bm_off);
                 nfull = 0;
             }
         }
@@ -875,31 +876,83 @@ Run *run_program(Context &ctx, int program, const int32_t *rows, u64 n, bool on_
     return r;
 }
 
+// Result rows [a, b) of a run into tmp + 2a (device memory). A bit-matrix
+// run's rows leave by units (TC column blocks, SG matrix rows): ua/ub are
+// then the units whose rows are [a, b).
+static void extract_range(Context &ctx, const Run &r, int32_t *tmp, u64 a, u64 b, u64 ua, u64 ub) {
+    const int32_t *ids = r.ids.as<int32_t>();
+    const u64 n = b - a;
+    if (r.from_bitmat) {
+        bitmat_extract_rows(ctx, r, tmp, ua, ub);
+        ctx.prof_add_bytes(K_BITMAP_EXTRACT, 8.0 * n);
+    } else if (r.program == DL_PROGRAM_WCC) {
+        DL_LAUNCH(ctx, K_PREP, 0, unpack_components_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(
+                                      r.aux.as<u32>() + a, n, ids, tmp + 2 * a));
+    } else if (r.program == DL_PROGRAM_SG) {
+        DL_LAUNCH(ctx, K_PREP, 0, unpack_rows_kernel<true><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(
+                                      r.words.as<u64>() + a, n, r.bits, ids, tmp + 2 * a));
+    } else {
+        DL_LAUNCH(ctx, K_PREP, 0, unpack_rows_kernel<false><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(
+                                      r.words.as<u64>() + a, n, r.bits, ids, tmp + 2 * a));
+    }
+    DL_CHECK_LAUNCH();
+}
+
 void run_copy_output(const Run &r, int32_t *dst, u64 capacity, bool dst_on_device) {
     Context &ctx = *r.ctx;
     const u64 n = (u64) r.info.output_rows;
     if (capacity < n) throw Error(DL_ERR_INVALID_ARGUMENT, "output capacity " + std::to_string(capacity) + " < " +
                                                                std::to_string(n) + " rows");
     if (n == 0) return;
-    int32_t *tmp = dst;
+    const u64 units = r.from_bitmat ? bitmat_units(r) : n;
+    if (dst_on_device) {
+        extract_range(ctx, r, dst, 0, n, 0, units);
+        ctx.sync();
+        return;
+    }
+    // Host destination: the rows are written to a device stage in chunks, and
+    // each chunk's copy to the host runs on a second stream while the next
+    // chunk is written.
     DevBuf stage;
-    if (!dst_on_device) {
-        ctx.reserve(stage, n * 8);
-        tmp = stage.as<int32_t>();
-    }
-    const int32_t *ids = r.ids.as<int32_t>();
+    ctx.reserve(stage, n * 8);
+    int32_t *tmp = stage.as<int32_t>();
+    const int kchunks = (int) std::min<u64>(n * 8 >= (256ull << 20) ? 8 : 1, units);
+    u64 *bound = ctx.host_scalars + 16;  // row bounds of the chunks (kchunks + 1 <= 9 slots)
+    std::vector<u64> ubound(kchunks + 1);
+    for (int k = 0; k <= kchunks; ++k) ubound[k] = units * k / kchunks;
     if (r.from_bitmat) {
-        bitmat_extract_rows(ctx, r, tmp);
-    } else if (r.program == DL_PROGRAM_WCC) {
-        DL_LAUNCH(ctx, K_PREP, 0, unpack_components_kernel<<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.aux.as<u32>(), n, ids, tmp));
-    } else if (r.program == DL_PROGRAM_SG) {
-        DL_LAUNCH(ctx, K_PREP, 0, unpack_rows_kernel<true><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.words.as<u64>(), n, r.bits, ids, tmp));
+        for (int k = 0; k <= kchunks; ++k) {
+            const u64 idx = bitmat_unit_index(r, ubound[k]);
+            if (idx >= r.bm_n) bound[k] = n;
+            else DL_CUDA(cudaMemcpyAsync(bound + k, r.bm_first.as<u64>() + idx, 8, cudaMemcpyDeviceToHost, ctx.stream));
+        }
+        ctx.sync();
     } else {
-        DL_LAUNCH(ctx, K_PREP, 0, unpack_rows_kernel<false><<<grid_for(n, T256, ctx), T256, 0, ctx.stream>>>(r.words.as<u64>(), n, r.bits, ids,
-                                                                                   tmp));
+        for (int k = 0; k <= kchunks; ++k) bound[k] = ubound[k];
     }
-    DL_CHECK_LAUNCH();
-    if (!dst_on_device) DL_CUDA(cudaMemcpyAsync(dst, tmp, n * 8, cudaMemcpyDeviceToHost, ctx.stream));
+    std::vector<u64> rows(bound, bound + kchunks + 1);
+    cudaStream_t cs = ctx.copy_stream_get();
+    std::vector<cudaEvent_t> ev(kchunks, nullptr);
+    try {
+        for (int k = 0; k < kchunks; ++k) {
+            if (rows[k + 1] <= rows[k]) continue;
+            extract_range(ctx, r, tmp, rows[k], rows[k + 1], ubound[k], ubound[k + 1]);
+            DL_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+            DL_CUDA(cudaEventRecord(ev[k], ctx.stream));
+            DL_CUDA(cudaStreamWaitEvent(cs, ev[k], 0));
+            DL_CUDA(cudaMemcpyAsync(dst + 2 * rows[k], tmp + 2 * rows[k], (rows[k + 1] - rows[k]) * 8,
+                                    cudaMemcpyDeviceToHost, cs));
+        }
+        DL_CUDA(cudaStreamSynchronize(cs));
+    } catch (...) {
+        cudaStreamSynchronize(cs);
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        ctx.give_back(stage);
+        throw;
+    }
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
     ctx.sync();
     ctx.give_back(stage);
 }
@@ -929,6 +982,7 @@ void run_destroy(Run *r) {
         r->ctx->give_back(r->labels);
         r->ctx->give_back(r->bm_t);
         r->ctx->give_back(r->bm_first);
+        r->ctx->give_back(r->bm_off);
     }
     delete r;
 }

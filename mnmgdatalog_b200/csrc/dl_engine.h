@@ -22,12 +22,15 @@ struct Run {
     DevBuf aux;               // WCC: component ranks, ascending
     u64 n_aux = 0;
     DevBuf labels;            // WCC: label rank of every node
-    // TC / SG on the bit matrix: the result stays as the matrix's transpose
-    // (TC: row = path target) or the matrix (SG) with each row's first output
-    // position; rows are extracted when they are copied out
+    // TC / SG on the bit matrix: the result stays as a matrix with each
+    // row's (or target's) first output position; rows are extracted when
+    // they are copied out. bm_t is TC's transpose (row = target), SG's
+    // matrix, or (bm_cols) TC's matrix itself with per (512-row block,
+    // target) offsets in bm_off.
     bool from_bitmat = false;
-    bool bm_row_first = false;  // SG: the matrix itself, rows (row id, column id)
-    DevBuf bm_t, bm_first;
+    bool bm_row_first = false;  // SG: rows (row id, column id) from the matrix rows
+    bool bm_cols = false;       // TC: rows from the matrix's columns
+    DevBuf bm_t, bm_first, bm_off;
     u64 bm_n = 0, bm_stride = 0, bm_words = 0;
 };
 
@@ -35,6 +38,8 @@ Run *run_program(Context &ctx, int program, const int32_t *rows, u64 n, bool on_
 void run_copy_output(const Run &r, int32_t *dst, u64 capacity, bool dst_on_device);
 void run_copy_labels(const Run &r, int32_t *node_ids, int32_t *labels, u64 capacity);
 void run_destroy(Run *r);
-void bitmat_extract_rows(Context &ctx, const Run &r, int32_t *out);
+u64 bitmat_units(const Run &r);
+u64 bitmat_unit_index(const Run &r, u64 unit);
+void bitmat_extract_rows(Context &ctx, const Run &r, int32_t *out, u64 u0, u64 u1);
 
 }  // namespace dl

@@ -101,9 +101,9 @@ void settle(Context &ctx, FullSet &F);
 
 // TC with full as an n x n bit matrix (dl_bitmap.cu).
 u64 bitmat_bytes(u64 n);
-// Whether a run over n node ranks keeps full as an n x n bit matrix:
-// `copies` matrices (TC 2: the matrix and its transpose; SG 1) must fit.
-bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, int copies);
+// Whether a run over n node ranks keeps full as an n x n bit matrix: the
+// matrix, and for TC (sg false) its result rows' column offsets, must fit.
+bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, bool sg);
 u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u64 ne, const dl_options &opt,
                        PhaseTimer &pt);
 // SG with full as a bit matrix; throws DL_ERR_OVERFLOW when a step's new rows

@@ -78,8 +78,8 @@ enum KernelId : int {
     K_HASH_INSERT,     // hash-set dedup: 8 B read + 32 B probe sector per word, 40 B per new word
     K_BITMAP_EXPAND,   // bit-matrix TC step: 4 B per delta row in and out + 16 B per unit in and out +
                        // 4 B edge target per join word
-    K_BITMAP_TRANSPOSE,  // bit-matrix transpose with per-target counts: 2 x matrix bytes
-    K_BITMAP_EXTRACT,  // result rows from the transposed matrix: matrix read + 8 B per result row (+ count scan)
+    K_BITMAP_COLUMNS,    // per (row block, target) counts of the bit matrix and their column offsets
+    K_BITMAP_EXTRACT,  // result rows from the bit matrix: matrix (+ TC offsets) read + 8 B per result row (+ count scan)
     // host-side costs, counted with or without profiling (seconds = host wall time)
     K_HOST_MALLOC,     // cudaMalloc of a buffer that had to grow (bytes = size)
     K_HOST_FREE,       // cudaFree of a cached buffer dropped from the cache
@@ -110,7 +110,7 @@ struct Workspace {
     DevBuf offsets;        // join count offsets
     DevBuf offsets_next;   // bit-matrix TC: the next delta's join offsets
     DevBuf wcc_label, wcc_flag, wcc_next;
-    DevBuf bitmat[2];      // TC full relation as a bit matrix; its transpose
+    DevBuf bitmat[2];      // full relation as a bit matrix; TC's column offsets of the result rows
     DevBuf bit_hasout;     // bit-matrix TC: nodes with out-edges (one bit each)
 };
 
@@ -126,9 +126,10 @@ struct Tuning {
     u64 dense_ratio = 4;        // fused full rewrite when |J| * dense_ratio >= |large run|
     u64 small_ratio = 4;        // small run folded when |small| * small_ratio >= |large run|
     double hash_load = 0.5;     // default load factor of dl_build_hash_table
-    int bitmap_max_gib = 48;    // TC dedup AUTO: bit matrix and transpose at most this many GiB (0 = never)
+    int bitmap_max_gib = 48;    // TC dedup AUTO: bit matrix (+ its column offsets) at most this many GiB (0 = never)
     u32 bitmap_unit_rows = 65536;  // bit-matrix TC: delta rows per unit (one shared-memory row fold each)
     int cache_max_gib = 96;        // cached spare buffers of the context, at most this many GiB
+    int bitmap_result = 0;         // bit-matrix TC result: 0 transpose when it fits, else columns; 1 transpose; 2 columns
 };
 Tuning default_tuning();
 
@@ -137,6 +138,7 @@ struct Context {
     Tuning tune = default_tuning();
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t copy_stream = nullptr;  // result copies to the host beside `stream` (created on first use)
     int sm_count = 148;
     bool no_alloc = false;          // every buffer is a fixed slice; a new allocation is an internal error
     Ctrl *ctrl = nullptr;           // device control block
@@ -183,6 +185,7 @@ struct Context {
     // cached buffer and tries once more (with `minimum` bytes if given).
     void allocate(DevBuf &buf, size_t bytes, bool zero = false, size_t minimum = 0);
     void release_all();
+    cudaStream_t copy_stream_get();
 
     // Next look-back epoch; clears the look-back buffer when the 14-bit epoch
     // wraps so that no stale word can alias the current launch.

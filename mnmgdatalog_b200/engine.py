@@ -141,7 +141,7 @@ class Engine:
 
     TUNING_FIELDS = ("sort_algorithm", "sort_ranking", "sort_keys_per_thread", "sort_input_tma", "dense_ratio",
                      "small_ratio", "hash_load_factor", "join_first_pass", "bitmap_max_gib",
-                     "bitmap_unit_rows", "cache_max_gib")
+                     "bitmap_unit_rows", "cache_max_gib", "bitmap_result")
 
     def tuning(self) -> dict:
         """The context's engine knobs (dl_tuning)."""

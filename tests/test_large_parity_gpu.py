@@ -63,12 +63,19 @@ COUNT_CASES = sorted(c for c, v in REF.items() if not v["rows_sha256"])
 @pytest.mark.parametrize("case", ROW_CASES)
 def test_rows_equal_reference(engine, case):
     ref = REF[case]
-    modes = ["auto", "sort"] if ref["program"] == "tc" else ["auto"]
-    for dedup in modes:
-        r = engine.run(ref["program"], _load(case), dedup=dedup)
-        _check_counts(case, r)
-        assert _sha(r.rows) == ref["rows_sha256"], f"{case} ({dedup}): rows differ from the reference's file"
-        del r
+    # TC: the bit matrix with its result through the transpose and from its
+    # columns, and the sorted runs
+    modes = [("auto", 1), ("auto", 2), ("sort", 0)] if ref["program"] == "tc" else [("auto", 0)]
+    before = engine.tuning()
+    try:
+        for dedup, form in modes:
+            engine.set_tuning(bitmap_result=form)
+            r = engine.run(ref["program"], _load(case), dedup=dedup)
+            _check_counts(case, r)
+            assert _sha(r.rows) == ref["rows_sha256"], f"{case} ({dedup}, {form}): rows differ from the reference's file"
+            del r
+    finally:
+        engine.set_tuning(before)
     engine.release_memory()
 
 

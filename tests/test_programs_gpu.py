@@ -218,6 +218,31 @@ def test_tc_bitmap_max_iterations_and_selection(engine):
         engine.set_tuning(before)
 
 
+@pytest.mark.parametrize("form", [1, 2])
+def test_tc_bitmap_result_forms(engine, form):
+    """The bit-matrix TC result through the matrix's transpose (1) and from
+    its columns with per-block offsets (2): the same rows as the sort path,
+    to host and device memory, with dense and sparse id ranges, node counts
+    on and off the 512 / 1024 tile edges."""
+    import torch
+    from mnmgdatalog_b200 import graphs
+    before = engine.tuning()
+    inputs = [e for _, e in EDGE_CASES]
+    inputs += [graphs.chung_lu(n=n, m=3 * n, seed=n) for n in (511, 1024, 1537, 5000)]
+    inputs += [load_input(f) for f in TC_FILES if len(load_input(f)) <= 40000][:4]
+    try:
+        engine.set_tuning(bitmap_result=form)
+        for k, e in enumerate(inputs):
+            a = engine.tc(e, dedup="sort")
+            b = engine.tc(e, dedup="bitmap")
+            assert a.deltas.tolist() == b.deltas.tolist(), k
+            assert np.array_equal(a.rows, b.rows), k
+            d = engine.tc(torch.from_numpy(e).cuda(), dedup="bitmap", output="device")
+            assert np.array_equal(d.rows.cpu().numpy(), a.rows), k
+    finally:
+        engine.set_tuning(before)
+
+
 @pytest.mark.parametrize("unit_rows", [1, 7, 65536])
 def test_sg_bitmap_agrees_with_sorted_runs(engine, unit_rows):
     """SG on the bit matrix (the base rule's units (p, {p}), one fold per
