@@ -958,12 +958,35 @@ __global__ void column_offsets_kernel(u32 *__restrict__ off, u64 n, u64 xblocks,
     tot[z] = run;
 }
 
-// Row w of the matrix -> result rows (ids[w], ids[x]) for its set bits x,
-// ascending, from out[first[w]] on (SG's order: (x, y) sorted by (x, y)).
-// One warp per row; a lane takes 4 consecutive words per step (one 16-byte
-// load, the next one in flight); a step's rows are staged in shared memory
-// and leave with consecutive stores unless there are more than EX_STAGE of
-// them. (Result words are sparse, so each lane walks its own words' bits.)
+// Position of the k-th set bit (k from 0) of w, which has more than k set
+// bits: a binary search on the popcounts of the low halves.
+__device__ __forceinline__ u32 select_bit(u32 w, u32 k) {
+    u32 pos = 0, c;
+    c = __popc(w & 0xFFFFu);
+    if (k >= c) { k -= c; w >>= 16; pos += 16; }
+    c = __popc(w & 0xFFu);
+    if (k >= c) { k -= c; w >>= 8; pos += 8; }
+    c = __popc(w & 0xFu);
+    if (k >= c) { k -= c; w >>= 4; pos += 4; }
+    c = __popc(w & 0x3u);
+    if (k >= c) { k -= c; w >>= 2; pos += 2; }
+    if (k >= (w & 1u)) pos += 1;
+    return pos;
+}
+
+// Row w of the matrix -> result rows for its set bits x, ascending, from
+// out[first[w]] on: (ids[w], ids[x]) for SG's matrix (its order (x, y) by
+// (x, y)), (ids[x], ids[w]) for TC's transpose (row = target z: (x, z) by
+// (z, x)). One warp per row; a lane takes 4 consecutive words per step (one
+// 16-byte load, two steps' loads in flight). A sparse step (at most EX_STAGE
+// rows) is written by word: each lane walks its words' bits into a
+// shared-memory stage, which leaves with consecutive stores. A dense step is
+// written by output position: lane i writes rows i, i + 32, ... of the step,
+// finding the lane that holds the row by a binary search over the warp's
+// prefix counts and the bit inside its word by popcounts, so every lane
+// writes a row per pass and the stores are consecutive. (Measured: by word
+// is faster on TC's sparse transpose rows, by position 2.4x faster on SG's
+// dense rows.)
 constexpr int EX_THREADS = 256;
 constexpr int EX_STAGE = 256;
 template <bool RowFirst>
@@ -983,7 +1006,6 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u
         // a dense id range needs no table lookup (ids[r] == base + r)
         const u32 idw = (u32) (affine ? (int32_t) (base + (int64_t) w) : ids[w]);
         // stride is a multiple of 32 words: a lane's vector stays in the row.
-        // Two steps' loads are in flight while a step is emitted.
         auto load = [&](u64 k) {
             return k < words ? __ldcs(reinterpret_cast<const uint4 *>(row + k)) : make_uint4(0, 0, 0, 0);
         };
@@ -1001,8 +1023,9 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u
             const u32 incl = warp_inclusive_sum(cnt);
             const u32 sum = __shfl_sync(0xffffffffu, incl, 31);
             if (sum == 0) continue;
-            u32 p = incl - cnt;
+            const u32 excl = incl - cnt;
             if (sum <= EX_STAGE) {
+                u32 p = excl;
 #pragma unroll
                 for (int c = 0; c < 4; ++c)
                     for (u32 b = v[c]; b; b &= b - 1)
@@ -1010,12 +1033,28 @@ __global__ void __launch_bounds__(EX_THREADS) bitmat_extract_rows_kernel(const u
                 __syncwarp();
                 for (u32 i = lane; i < sum; i += 32) out[pos + i] = st[i];
                 __syncwarp();
-            } else {
-                u64 q2 = pos + p;
+                pos += sum;
+                continue;
+            }
+            for (u32 r0 = 0; r0 < sum; r0 += 32) {
+                const u32 r = r0 + lane;
+                // owner: the last lane whose exclusive prefix is <= r (it
+                // holds row r whenever r < sum)
+                u32 L = 0;
 #pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    for (u32 b = v[c]; b; b &= b - 1)
-                        out[q2++] = pack_row<RowFirst>(idw, xid(ids, affine, base, (k + c) * 32 + (__ffs(b) - 1)));
+                for (u32 step = 16; step >= 1; step >>= 1)
+                    if (__shfl_sync(0xffffffffu, excl, L + step) <= r) L += step;
+                u32 kk = r - __shfl_sync(0xffffffffu, excl, L);
+                const u32 w0 = __shfl_sync(0xffffffffu, v[0], L), w1 = __shfl_sync(0xffffffffu, v[1], L);
+                const u32 w2 = __shfl_sync(0xffffffffu, v[2], L), w3 = __shfl_sync(0xffffffffu, v[3], L);
+                u32 c = 0, word = w0, pc = __popc(w0);
+                if (kk >= pc) { kk -= pc; c = 1; word = w1; pc = __popc(w1); }
+                if (c == 1 && kk >= pc) { kk -= pc; c = 2; word = w2; pc = __popc(w2); }
+                if (c == 2 && kk >= pc) { kk -= pc; c = 3; word = w3; }
+                if (r < sum) {
+                    const u64 x = (k0 + 4 * L + c) * 32 + select_bit(word, kk);
+                    out[pos + r] = pack_row<RowFirst>(idw, xid(ids, affine, base, x));
+                }
             }
             pos += sum;
         }

@@ -78,7 +78,8 @@ enum KernelId : int {
     K_HASH_INSERT,     // hash-set dedup: 8 B read + 32 B probe sector per word, 40 B per new word
     K_BITMAP_EXPAND,   // bit-matrix TC step: 4 B per delta row in and out + 16 B per unit in and out +
                        // 4 B edge target per join word
-    K_BITMAP_COLUMNS,    // per (row block, target) counts of the bit matrix and their column offsets
+    K_BITMAP_COLUMNS,  // TC result set-up from the bit matrix: its transpose with per-target counts
+                       // (2 x matrix), or per (row block, target) counts and their offsets
     K_BITMAP_EXTRACT,  // result rows from the bit matrix: matrix (+ TC offsets) read + 8 B per result row (+ count scan)
     // host-side costs, counted with or without profiling (seconds = host wall time)
     K_HOST_MALLOC,     // cudaMalloc of a buffer that had to grow (bytes = size)

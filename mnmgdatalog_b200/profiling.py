@@ -31,7 +31,7 @@ CLASSES = [
     (r"digit0_hist_kernel", "join_count_scan"),
     (r"bucket_starts_kernel", "join_partition"),
     (r"bitmat_unit_step_kernel|bitmat_set_edges_kernel", "bitmap_expand"),
-    (r"bitmat_column_count|column_offsets", "bitmap_columns"),
+    (r"bitmat_transpose_count|bitmat_column_count|column_offsets", "bitmap_columns"),
     (r"bitmat_extract|bitmat_column_rows|scan_kernel<.*CountValue", "bitmap_extract"),
     (r"lbs_partition_kernel", "join_partition"),
     (r"select_kernel", "select_compact"),
