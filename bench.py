@@ -80,7 +80,12 @@ def measured_peak_gbs() -> tuple[float, str]:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
+
+    nvidia-smi is started before the warm-up (its start-up queries the driver
+    for a while, which is kept out of the timed steps); mark() and stop()
+    bracket the timed region, and only samples taken in between count (the
+    nearest later one if none landed inside)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -89,7 +94,8 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.lines: list[str] = []
+        self.lines: list[tuple[float, str]] = []
+        self.t_mark = None
 
     def start(self):
         exe = shutil.which("nvidia-smi")
@@ -103,20 +109,33 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def mark(self):
+        """The timed region starts."""
+        self.t_mark = time.monotonic()
 
     def stop(self) -> dict:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        t_end = time.monotonic()
+        # at least one sample from the timed region or just after it
+        deadline = t_end + 2.0
+        while time.monotonic() < deadline and not any(t >= (self.t_mark or 0) for t, _ in self.lines):
+            time.sleep(0.05)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.thread.join(timeout=2)
+        t0 = self.t_mark or 0.0
+        inside = [ln for t, ln in self.lines if t0 <= t <= t_end]
+        if not inside:
+            inside = [ln for t, ln in self.lines if t >= t0][:1]
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in inside:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -235,13 +254,15 @@ def timed_fixpoints(eng, prog, d_edges, steps, warmup, dedup, dev, world, barrie
     def step():
         return eng.run(prog, d_edges, output="device", out=out_rows, dedup=dedup)
 
+    if clocks:
+        clocks.start()  # before the warm-up: nvidia-smi's start-up stays out of the timed steps
     for _ in range(warmup):
         step()
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
     if clocks:
-        clocks.start()
+        clocks.mark()
     eng.profile(True)
     stream = eng._stream_obj
     evs = []
