@@ -1331,6 +1331,10 @@ u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &o
     const u64 resident = (u64) ctx.sm_count * std::max(small ? per_sm_s : per_sm, 1);
     u64 nfull = 0;
     int slot = 0;
+    // the free device memory, read once: a driver query per iteration costs
+    // more than many of SG's small steps
+    size_t free_b = 0, total_b = 0;
+    DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
     for (int it = 0;; ++it) {  // it 0: the base rule (sg.cu:170-217); then sg.cu:244-390
         pt.mark(it == 0 ? PH_INIT : PH_JOIN);
         u64 nnew = 0, next_units = 0, next_rows = 0, next_bound = 0;
@@ -1342,11 +1346,9 @@ u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &o
             // behind). The buffer is also capped by the device memory left; a
             // step that overflows it reports DL_DEVERR_CAPACITY and the caller
             // reruns the program on the sorted runs.
-            size_t free_b = 0, total_b = 0;
-            DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
             const u64 need = bound + bound / 3 + warps * WCHUNK;
-            // rows (8 B) at most 1/16 of the free memory, unit slots (16 B, at
-            // most one per row) at most 1/8
+            // rows (8 B) at most 1/16 of the memory free at the start, unit
+            // slots (16 B, at most one per row) at most 1/8
             const u64 cap_rows = std::max<u64>(warps * WCHUNK, (u64) free_b / 16 / 8);
             const u64 ocap = std::min(need, cap_rows);
             DevBuf &obuf = ws.jbuf[slot];
