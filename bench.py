@@ -591,6 +591,17 @@ def measure_batched(eng, dev, args) -> dict:
         eng.synchronize()
         times.append(time.perf_counter() - t0)
     t_batch = statistics.median(times)
+    # one more batched run under the live profile (outside the timing): the
+    # sorted-runs kernels' shares and roofline fractions on this workload
+    eng.profile(True)
+    t0 = time.perf_counter()
+    for p, g in groups.items():
+        eng.run_batch(p, g, output="none")
+    eng.synchronize()
+    t_prof = time.perf_counter() - t0
+    prof = eng.profile_read()
+    eng.profile(False)
+    b_roofline, b_kernels, b_host, b_launches = roofline_of(prof, t_prof)
     t0 = time.perf_counter()
     plain = {p: [eng.run(p, x, output="none") for x in g] for p, g in groups.items()}
     eng.synchronize()
@@ -609,6 +620,8 @@ def measure_batched(eng, dev, args) -> dict:
             "reps": reps, "batch_seconds": {"median": t_batch, "min": min(times), "max": max(times)},
             "queries_per_s_range": [n / max(times), n / min(times)],
             "identical_to_plain": bool(same), "tuning": tuned, "tuning_source": source,
+            "roofline": b_roofline, "kernels": b_kernels, "host": b_host, "gpu_launches": b_launches,
+            "profiled_run": "one extra batched run under the live profile, outside the timing",
             "timer": "host wall clock around dl_run_batch per program (synchronized), inputs in HBM",
             "form": "union fixpoint per program (one launch sequence per iteration for all instances)"}
 

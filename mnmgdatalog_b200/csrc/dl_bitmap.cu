@@ -747,6 +747,7 @@ constexpr int CX_XW = CX_ROWS / 32;           // words of a target row in a tile
 constexpr int CX_THREADS = 512;
 struct ColSmem {
     u32 in[2][CX_ROWS][CX_WORDS];  // source tiles (two buffers)
+    u32 live[2][CX_ROWS / 32];     // the tiles' row-written bits
     u32 outw[CX_TARGETS][CX_XW];   // the current tile, target-major
     u64 base[CX_TARGETS];          // rows pass: first output row of each target in this tile
     u32 cnt[CX_TARGETS];           // count pass: set bits of each target in this tile
@@ -756,7 +757,8 @@ static_assert(CX_WORDS == 32 && CX_ROWS / 32 == CX_THREADS / 32, "one block per 
 enum ColMode { COL_COUNT = 0, COL_ROWS = 1, COL_TRANSPOSE = 2 };
 
 template <int MODE>
-__device__ __forceinline__ void bitmat_columns_body(const u32 *__restrict__ m, u64 n, u64 stride, u64 xblocks,
+__device__ __forceinline__ void bitmat_columns_body(const u32 *__restrict__ m, const u32 *__restrict__ live,
+                                                    u64 n, u64 stride, u64 xblocks,
                                                     u64 t_first, u64 tiles, u32 *__restrict__ off,
                                                     const u64 *__restrict__ first,
                                                     const int32_t *__restrict__ ids, bool affine, int32_t base,
@@ -780,6 +782,8 @@ __device__ __forceinline__ void bitmat_columns_body(const u32 *__restrict__ m, u
             if (x0 + r < n) cp_async16(dst, src + (x0 + r) * stride + c4 * 4);
             else *reinterpret_cast<uint4 *>(dst) = make_uint4(0u, 0u, 0u, 0u);
         }
+        // the tile's 16 words of `live` (padded to whole tiles by the caller)
+        if (tid < CX_ROWS / 32 / 4) cp_async16(&s.live[buf][4 * tid], live + x0 / 32 + 4 * tid);
     };
     const u32 rb = lane & 15, cw = (warp + lane) & 31, hi = lane >> 4;
     const u32 q = tid & 3;  // this thread's quarter of a target row
@@ -832,9 +836,12 @@ __device__ __forceinline__ void bitmat_columns_body(const u32 *__restrict__ m, u
             // counts only: rotate row words right by `lane` before the
             // transpose, so that a[b] then belongs to target 32 cw + (b + lane)
             // % 32 and the 32 lanes' shared-memory atomics hit 32 banks
+            // rows the fixpoint never wrote (sources without out-edges: not
+            // zeroed, they may hold an earlier run's bits) read as zero
+            const u32 lw = s.live[buf][rb];
 #pragma unroll
             for (int r = 0; r < 32; ++r) {
-                const u32 w = s.in[buf][32 * rb + r][cw];
+                const u32 w = ((lw >> r) & 1u) ? s.in[buf][32 * rb + r][cw] : 0u;
                 a[r] = __funnelshift_r(w, w, lane);
             }
             transpose32_regs(a);
@@ -854,8 +861,9 @@ __device__ __forceinline__ void bitmat_columns_body(const u32 *__restrict__ m, u
 #pragma unroll
                 for (int k = 0; k < CX_TARGETS / CX_THREADS; ++k) s.base[tid + k * CX_THREADS] = pb[k];
             }
+            const u32 lw = s.live[buf][rb];  // unwritten rows read as zero
 #pragma unroll
-            for (int r = 0; r < 32; ++r) a[r] = s.in[buf][32 * rb + r][cw];
+            for (int r = 0; r < 32; ++r) a[r] = ((lw >> r) & 1u) ? s.in[buf][32 * rb + r][cw] : 0u;
             transpose32_regs(a);
             // a[b] = word rb of target 32 cw + b; the upper half-warp stores
             // b ^ 1 while the lower stores b, so the 32 stores hit 32 banks
@@ -911,27 +919,41 @@ __device__ __forceinline__ void bitmat_columns_body(const u32 *__restrict__ m, u
 }
 
 __global__ void __launch_bounds__(CX_THREADS, 1)
-bitmat_column_count_kernel(const u32 *__restrict__ m, u64 n, u64 stride, u64 xblocks, u64 tiles,
-                           u32 *__restrict__ off) {
-    bitmat_columns_body<COL_COUNT>(m, n, stride, xblocks, 0, tiles, off, nullptr, nullptr, false, 0, nullptr,
+bitmat_column_count_kernel(const u32 *__restrict__ m, const u32 *__restrict__ live, u64 n, u64 stride, u64 xblocks,
+                           u64 tiles, u32 *__restrict__ off) {
+    bitmat_columns_body<COL_COUNT>(m, live, n, stride, xblocks, 0, tiles, off, nullptr, nullptr, false, 0, nullptr,
                                    nullptr, nullptr);
 }
 
 __global__ void __launch_bounds__(CX_THREADS, 1)
-bitmat_column_rows_kernel(const u32 *__restrict__ m, u64 n, u64 stride, u64 xblocks, u64 t_first, u64 tiles,
-                          const u32 *__restrict__ off, const u64 *__restrict__ first,
+bitmat_column_rows_kernel(const u32 *__restrict__ m, const u32 *__restrict__ live, u64 n, u64 stride, u64 xblocks,
+                          u64 t_first, u64 tiles, const u32 *__restrict__ off, const u64 *__restrict__ first,
                           const int32_t *__restrict__ ids, bool affine, int32_t base, u64 *__restrict__ out) {
-    bitmat_columns_body<COL_ROWS>(m, n, stride, xblocks, t_first, tiles, const_cast<u32 *>(off), first, ids, affine,
-                                  base, out, nullptr, nullptr);
+    bitmat_columns_body<COL_ROWS>(m, live, n, stride, xblocks, t_first, tiles, const_cast<u32 *>(off), first, ids,
+                                  affine, base, out, nullptr, nullptr);
 }
 
-// t = the transpose of m (n rows of `stride` words each), counts[z] += the
-// set bits of row z of t (counts zeroed by the caller).
+// t = the transpose of m (n rows of `stride` words each; rows whose bit in
+// `live` is clear read as zero), counts[z] += the set bits of row z of t
+// (counts zeroed by the caller).
 __global__ void __launch_bounds__(CX_THREADS, 1)
-bitmat_transpose_count_kernel(const u32 *__restrict__ m, u64 n, u64 stride, u64 xblocks, u64 tiles,
-                              u32 *__restrict__ t, unsigned long long *__restrict__ counts) {
-    bitmat_columns_body<COL_TRANSPOSE>(m, n, stride, xblocks, 0, tiles, nullptr, nullptr, nullptr, false, 0, nullptr,
-                                       t, counts);
+bitmat_transpose_count_kernel(const u32 *__restrict__ m, const u32 *__restrict__ live, u64 n, u64 stride,
+                              u64 xblocks, u64 tiles, u32 *__restrict__ t, unsigned long long *__restrict__ counts) {
+    bitmat_columns_body<COL_TRANSPOSE>(m, live, n, stride, xblocks, 0, tiles, nullptr, nullptr, nullptr, false, 0,
+                                       nullptr, t, counts);
+}
+
+// Zero the rows of m whose bit in `live` is set (one warp per row, 16-byte
+// stores): TC writes only the rows of sources with out-edges, and readers of
+// the matrix treat the other rows as zero.
+__global__ void bitmat_zero_rows_kernel(u32 *__restrict__ m, u64 n, u64 stride, const u32 *__restrict__ live) {
+    const u64 warps = (u64) gridDim.x * (blockDim.x / 32);
+    const u32 lane = threadIdx.x & 31;
+    for (u64 x = (u64) blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); x < n; x += warps) {
+        if (!((__ldg(live + (x >> 5)) >> (x & 31)) & 1u)) continue;
+        uint4 *row = reinterpret_cast<uint4 *>(m + x * stride);
+        for (u64 k = lane; k < stride / 4; k += 32) row[k] = make_uint4(0u, 0u, 0u, 0u);
+    }
 }
 
 // off[.][z]: per row block counts of column z -> exclusive prefix over the
@@ -1135,8 +1157,18 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
                                                               " nodes do not fit in shared memory");
     DevBuf &M = ws.bitmat[0];
     ctx.reserve(M, std::max<u64>(bitmat_bytes(n), 4));
-    DL_CUDA(cudaMemsetAsync(M.p, 0, bitmat_bytes(n), ctx.stream));
     u32 *m = M.as<u32>();
+    // sources with out-edges: the only rows the fixpoint writes (every unit's
+    // source has out-edges), so only they are zeroed; the other rows are
+    // read as zero by the result's kernels
+    // (padded to whole 512-row tiles: the result's kernels read a tile's 16 words at once)
+    ctx.reserve(ws.bit_hasout, ((words_used + 15) / 16 * 16 + 16) * 4);
+    DL_LAUNCH(ctx, K_PREP, 4.0 * n + 4.0 * words_used,
+              hasout_kernel<<<grid_for(words_used, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, words_used,
+                                                                                      ws.bit_hasout.as<u32>()));
+    DL_LAUNCH(ctx, K_PREP, 0,
+              bitmat_zero_rows_kernel<<<grid_for(n * 32, T256, ctx, 8), T256, 0, ctx.stream>>>(
+                  m, n, stride, ws.bit_hasout.as<u32>()));
     StepCounters *ctr = reinterpret_cast<StepCounters *>(&ctx.ctrl->scalar[52]);
     // delta_0 = the edges: one row per CSR value (its edge range), units from
     // the CSR's offsets; the rows live in jbuf[1], the first step writes jbuf[0]
@@ -1170,10 +1202,6 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
         ctx.sync();
         join = ctx.host_scalars[0];
     }
-    ctx.reserve(ws.bit_hasout, std::max<u64>(words_used, 1) * 4);
-    DL_LAUNCH(ctx, K_PREP, 4.0 * n + 4.0 * words_used,
-              hasout_kernel<<<grid_for(words_used, T256, ctx), T256, 0, ctx.stream>>>(g.csr.off, n, words_used,
-                                                                                      ws.bit_hasout.as<u32>()));
     u64 nfull = ne;
     u64 nrows = ne;  // rows of the current delta
     auto kern = bitmat_unit_step_kernel;
@@ -1251,14 +1279,15 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
                                          (int) sizeof(ColSmem)));
             DL_LAUNCH(ctx, K_BITMAP_COLUMNS, 2.0 * bitmat_bytes(n),
                       bitmat_transpose_count_kernel<<<cg, CX_THREADS, sizeof(ColSmem), ctx.stream>>>(
-                          m, n, stride, xblocks, tiles, O.as<u32>(), reinterpret_cast<unsigned long long *>(counts)));
+                          m, ws.bit_hasout.as<u32>(), n, stride, xblocks, tiles, O.as<u32>(),
+                          reinterpret_cast<unsigned long long *>(counts)));
         } else {
             ctx.reserve(O, bitmat_column_offset_bytes(n));
             DL_CUDA(cudaFuncSetAttribute(bitmat_column_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int) sizeof(ColSmem)));
             DL_LAUNCH(ctx, K_BITMAP_COLUMNS, 1.0 * bitmat_bytes(n) + 4.0 * xblocks * n,
                       bitmat_column_count_kernel<<<cg, CX_THREADS, sizeof(ColSmem), ctx.stream>>>(
-                          m, n, stride, xblocks, tiles, O.as<u32>()));
+                          m, ws.bit_hasout.as<u32>(), n, stride, xblocks, tiles, O.as<u32>()));
             DL_LAUNCH(ctx, K_BITMAP_COLUMNS, 8.0 * xblocks * n + 8.0 * n,
                       column_offsets_kernel<<<grid_for(n, T256, ctx, 64), T256, 0, ctx.stream>>>(
                           O.as<u32>(), n, xblocks, reinterpret_cast<unsigned long long *>(counts)));
@@ -1274,6 +1303,8 @@ u64 tc_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const u64 *edges, u
             r.bm_t = M;
             M = DevBuf();
             r.bm_off = O;
+            r.bm_live = ws.bit_hasout;  // the rows pass reads M again when the rows are copied out
+            ws.bit_hasout = DevBuf();
             r.bm_cols = true;
         }
         O = DevBuf();
@@ -1475,7 +1506,8 @@ void bitmat_extract_rows(Context &ctx, const Run &r, int32_t *out, u64 u0, u64 u
     // (the rows' 8 bytes each are added by the caller)
     DL_LAUNCH(ctx, K_BITMAP_EXTRACT, 128.0 * xblocks * CX_ROWS * (u1 - u0) + 4.0 * xblocks * CX_TARGETS * (u1 - u0),
               bitmat_column_rows_kernel<<<cg, CX_THREADS, sizeof(ColSmem), ctx.stream>>>(
-                  r.bm_t.as<u32>(), n, r.bm_stride, xblocks, u0 * xblocks, tiles, r.bm_off.as<u32>(),
+                  r.bm_t.as<u32>(), r.bm_live.as<u32>(), n, r.bm_stride, xblocks, u0 * xblocks, tiles,
+                  r.bm_off.as<u32>(),
                   r.bm_first.as<u64>(), r.ids.as<int32_t>(), r.ids_affine, r.id_base, reinterpret_cast<u64 *>(out)));
 }
 

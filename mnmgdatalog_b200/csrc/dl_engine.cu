@@ -983,6 +983,7 @@ void run_destroy(Run *r) {
         r->ctx->give_back(r->bm_t);
         r->ctx->give_back(r->bm_first);
         r->ctx->give_back(r->bm_off);
+        r->ctx->give_back(r->bm_live);
     }
     delete r;
 }

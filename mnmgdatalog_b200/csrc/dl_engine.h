@@ -31,6 +31,7 @@ struct Run {
     bool bm_row_first = false;  // SG: rows (row id, column id) from the matrix rows
     bool bm_cols = false;       // TC: rows from the matrix's columns
     DevBuf bm_t, bm_first, bm_off;
+    DevBuf bm_live;             // TC column form: the matrix rows that were written (one bit per row)
     u64 bm_n = 0, bm_stride = 0, bm_words = 0;
 };
 

@@ -10,7 +10,9 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT, load_input
+from conftest import ROOT, load_expected, load_input, sha_rows
+
+EXP = load_expected()
 
 pytestmark = pytest.mark.gpu
 
@@ -76,6 +78,10 @@ def test_cli_programs(engine, tmp_path, fname, prog, suffix):
     assert int(csv[0]) == len(e) and int(csv[1]) == 1
     assert int(csv[2]) == ours.iterations and int(csv[3]) == ours.output_tuples
     assert np.array_equal(got, ours.rows)
+    # and the file against the reference's own output for this input
+    rec = EXP["inputs"].get(fname, {}).get(prog)
+    if rec and rec.get("rows_sha256"):
+        assert sha_rows(got) == rec["rows_sha256"]
     # job_run = 1 writes no file
     os.remove(str(inp) + suffix)
     _run(exe, [str(inp), "0", "0", "1"], tmp_path)

@@ -243,6 +243,32 @@ def test_tc_bitmap_result_forms(engine, form):
         engine.set_tuning(before)
 
 
+@pytest.mark.parametrize("form", [1, 2])
+def test_tc_bitmap_unwritten_rows_read_as_zero(engine, form):
+    """Only the matrix rows of sources with out-edges are zeroed and written;
+    a run after one that filled every row (same node count, so the same
+    matrix buffer and layout) must not see the earlier bits in the rows of its
+    sinks."""
+    rng = np.random.default_rng(11)
+    n = 3000
+    src = np.repeat(np.arange(n), 8)  # 8 random out-edges per node, plus a cycle: every row fills up
+    full = np.concatenate([np.stack([src, rng.integers(0, n, size=len(src))], 1),
+                           np.stack([np.arange(n), (np.arange(n) + 1) % n], 1)]).astype(np.int32)
+    half = rng.integers(0, n, size=(4000, 2)).astype(np.int32)
+    half[:, 0] = half[:, 0] % (n // 2)  # sources in the lower half only
+    half = np.concatenate([half, [[n - 1, n - 1]]]).astype(np.int32)  # same id range
+    before = engine.tuning()
+    try:
+        engine.set_tuning(bitmap_result=form)
+        assert engine.tc(full, dedup="bitmap").output_tuples == n * n
+        a = engine.tc(half, dedup="sort")
+        b = engine.tc(half, dedup="bitmap")
+        assert a.deltas.tolist() == b.deltas.tolist()
+        assert np.array_equal(a.rows, b.rows)
+    finally:
+        engine.set_tuning(before)
+
+
 @pytest.mark.parametrize("unit_rows", [1, 7, 65536])
 def test_sg_bitmap_agrees_with_sorted_runs(engine, unit_rows):
     """SG on the bit matrix (the base rule's units (p, {p}), one fold per
