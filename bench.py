@@ -21,6 +21,7 @@ graph family, rank 0 only.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import shutil
@@ -267,17 +268,25 @@ def timed_fixpoints(eng, prog, d_edges, steps, warmup, dedup, dev, world, barrie
     stream = eng._stream_obj
     evs = []
     r = None
-    for _ in range(steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(1)                      # L2 flush, outside the timed events
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-        r = step()
-        with torch.cuda.stream(stream):
-            b.record(stream)
-        evs.append((a, b))
-    torch.cuda.synchronize(dev)
+    # Python's cyclic garbage collector stays off while steps are timed: a
+    # full collection between two of a step's library calls leaves the GPU
+    # idle for tens of milliseconds inside the events
+    gc.collect()
+    gc.disable()
+    try:
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)                      # L2 flush, outside the timed events
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            r = step()
+            with torch.cuda.stream(stream):
+                b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize(dev)
+    finally:
+        gc.enable()
     barrier()
     torch.cuda.synchronize(dev)
     prof = eng.profile_read()
@@ -525,13 +534,18 @@ def measure_e2e(eng, prog, edges, args, dev, world, barrier) -> dict:
     steps = max(1, min(args.steps, 3))
     barrier()
     torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    tuples = 0
-    for _ in range(steps):
-        r = eng.run(prog, h_edges, output="host", out=out, dedup=args.dedup)
-        tuples += r.output_tuples
-    torch.cuda.synchronize(dev)
-    sec = time.perf_counter() - t0
+    gc.collect()
+    gc.disable()  # as in the device-timed steps: no collection inside the timing
+    try:
+        t0 = time.perf_counter()
+        tuples = 0
+        for _ in range(steps):
+            r = eng.run(prog, h_edges, output="host", out=out, dedup=args.dedup)
+            tuples += r.output_tuples
+        torch.cuda.synchronize(dev)
+        sec = time.perf_counter() - t0
+    finally:
+        gc.enable()
     sec, total = combine_ranks(sec, float(tuples), world, dev)
     return {"value": total / sec, "unit": UNIT,
             "h2d_bytes_per_step": int(edges.nbytes), "d2h_bytes_per_step": int(out_rows * 8),
@@ -586,10 +600,15 @@ def measure_batched(eng, dev, args) -> dict:
     reps = max(5, min(args.steps, 7))
     times = []
     for _ in range(reps):
-        t0 = time.perf_counter()
-        batched = {p: eng.run_batch(p, g, output="none") for p, g in groups.items()}
-        eng.synchronize()
-        times.append(time.perf_counter() - t0)
+        gc.collect()
+        gc.disable()  # no collection inside a timed repetition
+        try:
+            t0 = time.perf_counter()
+            batched = {p: eng.run_batch(p, g, output="none") for p, g in groups.items()}
+            eng.synchronize()
+            times.append(time.perf_counter() - t0)
+        finally:
+            gc.enable()
     t_batch = statistics.median(times)
     # one more batched run under the live profile (outside the timing): the
     # sorted-runs kernels' shares and roofline fractions on this workload
@@ -602,10 +621,15 @@ def measure_batched(eng, dev, args) -> dict:
     prof = eng.profile_read()
     eng.profile(False)
     b_roofline, b_kernels, b_host, b_launches = roofline_of(prof, t_prof)
-    t0 = time.perf_counter()
-    plain = {p: [eng.run(p, x, output="none") for x in g] for p, g in groups.items()}
-    eng.synchronize()
-    t_plain = time.perf_counter() - t0
+    gc.collect()
+    gc.disable()
+    try:
+        t0 = time.perf_counter()
+        plain = {p: [eng.run(p, x, output="none") for x in g] for p, g in groups.items()}
+        eng.synchronize()
+        t_plain = time.perf_counter() - t0
+    finally:
+        gc.enable()
     same = all(a.iterations == b.iterations and a.output_tuples == b.output_tuples
                and a.deltas.tolist() == b.deltas.tolist()
                for p in groups for a, b in zip(batched[p], plain[p]))

@@ -1116,6 +1116,11 @@ bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, bool sg) {
     if ((n + 31) / 32 * 4 * (sg ? 3 : 1) + sizeof(SgSmem<UW>) + 4096 > 227 * 1024) return false;
     // TC also keeps the per (row block, target) offsets of its result rows
     const u64 need = bitmat_bytes(n) + (sg ? 0 : bitmat_column_offset_bytes(n));
+    // a context that already holds the matrix buffer (a repeated run) needs
+    // no driver query: the memory is its own
+    if (opt.dedup == DL_DEDUP_AUTO && ctx.ws.bitmat[0].cap >= bitmat_bytes(n) &&
+        need <= ((u64) ctx.tune.bitmap_max_gib << 30))
+        return true;
     size_t free_b = 0, total_b = 0;
     DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const u64 held = ctx.ws.bitmat[0].cap + ctx.ws.bitmat[1].cap;
@@ -1138,6 +1143,10 @@ static bool tc_result_by_transpose(Context &ctx, u64 n) {
     if (ctx.tune.bitmap_result == 2) return false;
     const u64 need = bitmat_bytes(n);
     if (2 * need > ((u64) ctx.tune.bitmap_max_gib << 30)) return false;
+    // a buffer the context keeps that the transpose would reuse: no query
+    if (ctx.ws.bitmat[1].cap >= need) return true;
+    for (const DevBuf &b : ctx.spares)
+        if (b.cap >= need && b.cap <= 4 * need) return true;
     size_t free_b = 0, total_b = 0;
     DL_CUDA(cudaMemGetInfo(&free_b, &total_b));
     u64 cached = ctx.ws.bitmat[1].cap;
