@@ -680,6 +680,10 @@ def measure_served(eng, args, tuning=None) -> dict:
     # service that has been up for a while
     srv = serve.Server(eng, budget_bytes=SERVE_BUDGET, keep_results=False, concurrent=True, pinned=True,
                        tuning=tuning)
+    # the objects that exist now (requests, graphs, the library) are moved out
+    # of the collector's reach, so collections during serving stay short
+    gc.collect()
+    gc.freeze()
     try:
         srv.serve([serve.Request(r.id, r.program, r.edges) for r in reqs[:120]])  # warm-up
         sats = [srv.serve(fresh()) for _ in range(2)]
@@ -692,6 +696,7 @@ def measure_served(eng, args, tuning=None) -> dict:
         poi = srv.serve(stream)
     finally:
         srv.close()
+        gc.unfreeze()
     sp50, sp95, sp99, _ = serve.percentiles(svc)
     return {"workload": f"{len(reqs)} requests, TC/SG/WCC uniform, edges log-uniform 1K-500K "
                         f"({sum(len(r.edges) for r in reqs)} edges in all); every input distinct: one of "
