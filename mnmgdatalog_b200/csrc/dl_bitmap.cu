@@ -149,17 +149,19 @@ __device__ __forceinline__ u32 take_group(ExpandSmemT<NW> &s, u32 lane) {
 
 // Join words of unit U into the shared row: for every delta row (an edge
 // range: first edge, degree), OR bit w into row[] for each edge target w, and
-// set summary bit w / 1024 when the word w / 32 goes from zero to non-zero.
+// when the word w / 32 goes from zero to non-zero, set summary bit w / 1024
+// (LIST false) or append w / 32 to the touched-word list lk[*nlist] (LIST
+// true; one shared-memory atomic per warp and window).
 // Warps take groups of 32 rows; the next group's rows are loaded while the
 // current one is expanded, 32 join words at a time (the rows starting in a
 // window are a bit mask; a word's row is the number of rows started up to
 // its position), with the next window's edge-target load in flight before
 // the current window's shared-memory atomics. Called by every thread of the
 // CTA; s.next_group must be zero.
-template <int NW>
+template <bool LIST = false, int NW>
 __device__ __forceinline__ void expand_unit(ExpandSmemT<NW> &s, u32 *row, u32 *summ, const uint2 *__restrict__ rows,
                                             const u32 *__restrict__ val, const Unit &U, u32 lane, u32 warp, u32 lt,
-                                            u32 le) {
+                                            u32 le, u32 *lk = nullptr, u32 *nlist = nullptr) {
     u32 grp = take_group(s, lane);
     uint2 cur = make_uint2(0, 0);
     if (grp * 32 + lane < U.len) cur = rows[U.start + grp * 32 + lane];
@@ -203,7 +205,16 @@ __device__ __forceinline__ void expand_unit(ExpandSmemT<NW> &s, u32 *row, u32 *s
                     const u32 a = addr(i0 + 32);
                     if (i0 + 32 + lane < total) wn = __ldg(val + a);
                 }
-                if (have) {
+                if constexpr (LIST) {
+                    const bool first = have && atomicOr(&row[w >> 5], 1u << (w & 31)) == 0u;
+                    const u32 fm = __ballot_sync(0xffffffffu, first);
+                    if (fm) {
+                        u32 at = 0;
+                        if (lane == (u32) (__ffs(fm) - 1)) at = atomicAdd(nlist, (u32) __popc(fm));
+                        at = __shfl_sync(0xffffffffu, at, __ffs(fm) - 1);
+                        if (first) lk[at + __popc(fm & lt)] = w >> 5;
+                    }
+                } else if (have) {
                     const u32 old = atomicOr(&row[w >> 5], 1u << (w & 31));
                     if (old == 0) atomicOr(&summ[w >> 10], 1u << ((w >> 5) & 31));
                 }
@@ -455,8 +466,8 @@ struct SgSmem {
     u32 nlist;                       // touched words of R in the list
     u64 res[NW][4];                  // per warp: next-delta rows [cur, end), unit slots [cur, end)
     unsigned long long acc[NW][3];   // per warp: new tuples, next-step bound, rows written
-    // followed by: u32 row[words], u32 summ[swords], u32 lk[words], u32 lv[words]
-    // (the touched words of R as a list: index, value)
+    // followed by: u32 row[words], u32 lk[words] (the touched words of R,
+    // listed by the expansion in the order they were first touched)
 };
 
 constexpr u64 WCHUNK = 4096;  // next-delta rows a warp reserves at a time
@@ -477,11 +488,12 @@ __device__ __forceinline__ void sg_close_range(u64 *res, u32 x, u64 start, u64 l
     }
 }
 
-// NT threads per CTA: 512 for long rows; 128 (16 CTAs per SM) when rows are
-// short enough, so that the many small units of SG run in more, smaller CTAs
-// (a unit's barriers then hold 4 warps instead of 16).
+// NT threads per CTA: 512 for long rows; 128 (up to 12 CTAs per SM) when rows
+// are short enough, so that the many small units of SG run in more, smaller
+// CTAs (a unit's barriers then hold 4 warps instead of 16). The bound leaves
+// 40 registers a thread: at 32 the kernel spilled.
 template <int NT>
-__global__ void __launch_bounds__(NT, 2048 / NT)
+__global__ void __launch_bounds__(NT, 1536 / NT)
 sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, const uint2 *__restrict__ rows,
                     const Unit *__restrict__ units, u64 nunits, u32 *__restrict__ m, u64 stride, u32 words,
                     uint2 *__restrict__ out, u64 out_cap, Unit *__restrict__ uout, u64 uout_cap, u64 unit_rows,
@@ -490,15 +502,11 @@ sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, co
     constexpr int NW = NT / 32;
     SgSmem<NW> &s = *reinterpret_cast<SgSmem<NW> *>(smem_raw);
     u32 *row = reinterpret_cast<u32 *>(smem_raw + sizeof(SgSmem<NW>));
-    const u32 swords = (words + 31) / 32;
-    u32 *summ = row + words;
-    u32 *lk = summ + swords;
-    u32 *lv = lk + words;
+    u32 *lk = row + words;
     const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const u32 lt = lanemask_lt();
     const u32 le = lane == 31 ? ~0u : (2u << lane) - 1;
-    const u32 nchunks = (swords + SCHUNK - 1) / SCHUNK;
-    for (u32 k = tid; k < words + swords; k += NT) row[k] = 0;
+    for (u32 k = tid; k < words; k += NT) row[k] = 0;
     if (lane == 0) {
         s.res[warp][0] = s.res[warp][1] = s.res[warp][2] = s.res[warp][3] = 0;
         s.acc[warp][0] = s.acc[warp][1] = s.acc[warp][2] = 0;
@@ -513,26 +521,13 @@ sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, co
             s.cur = s.next;
             s.next_x = 0;
         }
-        __syncthreads();  // (1) unit known; row, summary, group and target counters are clear
+        __syncthreads();  // (1) unit known; row, list, group and target counters are clear
         const Unit U = s.cur;
         if (U.len == 0) break;
         if (tid == 0) s.next = fetch_unit(units, nunits, ctr);  // read only at the next barrier (1)
-        expand_unit(s.e, row, summ, rows, val, U, lane, warp, lt, le);
-        __syncthreads();  // (2) R is complete
-        // ---- the touched words of R as a list (index, value), any order ----
-        for (u32 sw = tid; sw < swords; sw += NT) {
-            u32 bits = summ[sw];
-            if (!bits) continue;
-            u32 at = atomicAdd(&s.nlist, (u32) __popc(bits));
-            while (bits) {
-                const u32 k = sw * 32 + (__ffs(bits) - 1);
-                bits &= bits - 1;
-                lk[at] = k;
-                lv[at] = row[k];
-                ++at;
-            }
-        }
-        __syncthreads();  // (3) the list is complete
+        // R, and the list of its touched words (any order)
+        expand_unit<true>(s.e, row, nullptr, rows, val, U, lane, warp, lt, le, lk, &s.nlist);
+        __syncthreads();  // (2) R and its list are complete
         const u32 nlist = s.nlist;
         // ---- fold R into every row x of a's out-edges; emit each x's new rows ----
         // A warp takes one x at a time and walks the list 32 words per step,
@@ -559,7 +554,7 @@ sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, co
             for (u32 c0 = 0; c0 < nlist; c0 += 32) {
                 const bool have = c0 + lane < nlist;
                 const u32 k = have ? lk[c0 + lane] : 0u;
-                u32 v = have ? lv[c0 + lane] : 0u;
+                u32 v = have ? row[k] : 0u;
                 if (k == self_word) v &= ~(1u << (x & 31));  // base rule: x != y
                 const u32 o = v ? atomicOr(&m[mrow + k], v) : ~0u;
                 const u32 f = v & ~o;
@@ -623,14 +618,10 @@ sg_unit_step_kernel(const u32 *__restrict__ off, const u32 *__restrict__ val, co
                 s.acc[warp][2] += rw;
             }
         }
-        __syncthreads();  // (4) every fold target is done with R
-        // ---- clear R and its summary (the list holds every touched word) ----
-        for (u32 i2 = tid; i2 < nlist; i2 += NT) {
-            const u32 k = lk[i2];
-            row[k] = 0;
-            summ[k >> 5] = 0;
-        }
-        if (tid == 0) s.nlist = 0;  // read again only after barrier (3)
+        __syncthreads();  // (3) every fold target is done with R
+        // ---- clear R (the list holds every touched word) ----
+        for (u32 i2 = tid; i2 < nlist; i2 += NT) row[lk[i2]] = 0;
+        if (tid == 0) s.nlist = 0;  // read again only after barrier (2)
         if (tid == 0) s.e.next_group = 0;  // read again only after barrier (1)
     }
     // Unused reserved unit slots become empty units (skipped by fetch_unit).
@@ -1113,7 +1104,7 @@ u64 bitmat_column_offset_bytes(u64 n) { return std::max<u64>((n + CX_ROWS - 1) /
 bool bitmat_choose(Context &ctx, const dl_options &opt, u64 n, bool sg) {
     if (opt.dedup != DL_DEDUP_AUTO && opt.dedup != DL_DEDUP_BITMAP) return false;
     // a row (TC), or a row and its touched-word list (SG), must fit in shared memory
-    if ((n + 31) / 32 * 4 * (sg ? 3 : 1) + sizeof(SgSmem<UW>) + 4096 > 227 * 1024) return false;
+    if ((n + 31) / 32 * 4 * (sg ? 2 : 1) + sizeof(SgSmem<UW>) + 4096 > 227 * 1024) return false;
     // TC also keeps the per (row block, target) offsets of its result rows
     const u64 need = bitmat_bytes(n) + (sg ? 0 : bitmat_column_offset_bytes(n));
     // a context that already holds the matrix buffer (a repeated run) needs
@@ -1333,7 +1324,7 @@ u64 sg_bitmap_fixpoint(Context &ctx, Run &r, const Graph &g, const dl_options &o
     const u64 stride = bitmat_stride(n);
     const u64 unit_rows = std::max<u64>(1, ctx.tune.bitmap_unit_rows);
     const u64 words_used = (n + 31) / 32;
-    const size_t row_smem = (3 * words_used + (words_used + 31) / 32) * 4 + 16;
+    const size_t row_smem = 2 * words_used * 4 + 16;  // R and its touched-word list
     const size_t smem = sizeof(SgSmem<UW>) + row_smem;
     if (smem > 227 * 1024) throw Error(DL_ERR_OUT_OF_MEMORY, "bit-matrix rows of " + std::to_string(n) +
                                                               " nodes do not fit in shared memory");
