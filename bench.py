@@ -688,7 +688,9 @@ def measure_served(eng, args, tuning=None) -> dict:
         srv.serve([serve.Request(r.id, r.program, r.edges) for r in reqs[:120]])  # warm-up
         sats = [srv.serve(fresh()) for _ in range(2)]
         sat = max(sats, key=lambda x: x.queries_per_s)
-        rate = 0.8 * sat.queries_per_s
+        # the Poisson load is 80% of the slower saturated run: the faster one
+        # is not sustained under arrivals spread over time on every box
+        rate = 0.8 * min(x.queries_per_s for x in sats)
         stream = fresh()
         arr = serve.poisson_arrivals(len(stream), rate, np.random.default_rng(1))
         for r, t in zip(stream, arr):
@@ -701,9 +703,10 @@ def measure_served(eng, args, tuning=None) -> dict:
     return {"workload": f"{len(reqs)} requests, TC/SG/WCC uniform, edges log-uniform 1K-500K "
                         f"({sum(len(r.edges) for r in reqs)} edges in all); every input distinct: one of "
                         f"{args.serve_pool} seeded graphs per program under the request's own seeded id map; "
-                        f"Poisson arrivals at 80% of capacity",
+                        f"Poisson arrivals at 80% of the slower saturated run",
             "plain_sample": f"every {every}th request ({len(sample)})",
-            "capacity_queries_per_s": sat.queries_per_s, "plain_queries_per_s": plain_qps,
+            "capacity_queries_per_s": sat.queries_per_s, "capacity_runs": [x.queries_per_s for x in sats],
+            "plain_queries_per_s": plain_qps,
             "speedup_vs_plain": sat.queries_per_s / plain_qps,
             "poisson_rate": rate, "poisson_queries_per_s": poi.queries_per_s,
             "latency_s": {"p50": poi.latency_p50, "p95": poi.latency_p95, "p99": poi.latency_p99,
@@ -713,7 +716,8 @@ def measure_served(eng, args, tuning=None) -> dict:
             "max_active": poi.max_active, "peak_device_bytes": poi.peak_device_bytes,
             "budget_bytes": poi.budget_bytes, "budget_waits": poi.waits_on_budget,
             "server": "continuous batching, one union session per program, one worker thread and stream per "
-                      "program; warmed with 120 requests; capacity = better of two saturated runs",
+                      "program; warmed with 120 requests; capacity = better of two saturated runs; Poisson load "
+                      "at 80% of the slower one",
             "tuning": tuning,
             "delivery": "result rows copied into reused page-locked host buffers (served and plain alike)",
             "timer": "host wall clock; latency = result rows on the host - arrival"}
