@@ -181,3 +181,14 @@ def test_concurrent_worker_error_surfaces():
     srv = serve.Server(backend=backend, concurrent=True)
     with pytest.raises(RuntimeError, match="device lost"):
         srv.serve(_requests(6, seed=7))
+
+
+def test_device_headroom_leaves_room_for_worker_caches(monkeypatch):
+    """The server's budget is capped by the device memory free at start less
+    every worker context's reuse cache and a margin."""
+    import torch
+    gib = 1 << 30
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda device=None: (100 * gib, 180 * gib))
+    assert serve.device_headroom(0, 3, 4) == (100 - 3 * 4 - 2) * gib
+    assert serve.device_headroom(0, 1, 96) == 2 * gib
+    assert serve.device_headroom(0, 30, 4) == 0  # never negative
