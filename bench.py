@@ -1,7 +1,7 @@
 """Benchmark: derived tuples/s per fixpoint of the B200 Datalog engine.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config c1_tc_chung_lu|c0_tc_dag|c2_sg_lattice]
+                    [--config tc_chung_lu_317k|tc_dag_5k|sg_lattice_55]
 
 Default workload (one step = one whole TC fixpoint, init through the last
 iteration): transitive closure of a seeded Chung-Lu power-law graph with 317K
@@ -63,11 +63,11 @@ def workload(config: str):
 
 
 def describe(config: str, edges: np.ndarray) -> dict:
-    d = {"c1_tc_chung_lu": "TC, Chung-Lu n=317000 gamma=2.5 m=1050000 (each edge once, seed 0)",
-         "c0_tc_dag": "TC, DAG n=5000 p=0.7 + 2000 short edges (seed 0)",
-         "c2_sg_lattice": "SG, 55^3 lattice 6-neighbour p=0.15 + 1% long edges (seed 0)",
-         "p1_tc_chung_lu_small": "TC, Chung-Lu n=40000 gamma=2.5 m=132500 (each edge once, seed 0)",
-         "p2_tc_chung_lu_medium": "TC, Chung-Lu n=80000 gamma=2.5 m=265000 (each edge once, seed 0)",
+    d = {"tc_chung_lu_317k": "TC, Chung-Lu n=317000 gamma=2.5 m=1050000 (each edge once, seed 0)",
+         "tc_dag_5k": "TC, DAG n=5000 p=0.7 + 2000 short edges (seed 0)",
+         "sg_lattice_55": "SG, 55^3 lattice 6-neighbour p=0.15 + 1% long edges (seed 0)",
+         "tc_chung_lu_40k": "TC, Chung-Lu n=40000 gamma=2.5 m=132500 (each edge once, seed 0)",
+         "tc_chung_lu_80k": "TC, Chung-Lu n=80000 gamma=2.5 m=265000 (each edge once, seed 0)",
          "sg_fe_body": "SG, the reference's fe_body input (data/data_163734.bin, 163,734 edges)"}
     return {"workload": d.get(config, config), "config": config, "input_rows": int(len(edges))}
 
@@ -729,7 +729,7 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", default="c1_tc_chung_lu")
+    ap.add_argument("--config", default="tc_chung_lu_317k")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true",

@@ -1,6 +1,6 @@
 """Autotuner of the engine's knobs (dl_tuning) on a sample workload.
 
-    python -m mnmgdatalog_b200.autotune [--config p1_tc_chung_lu_small] [--out tuning.json]
+    python -m mnmgdatalog_b200.autotune [--config tc_chung_lu_40k] [--out tuning.json]
 
 Times candidate settings on a sample workload -- the radix pass variant
 (three-kernel LSD or onesweep, shared-memory or ballot ranking, onesweep
@@ -142,7 +142,7 @@ def main(argv=None) -> int:
     from . import graphs
     from .engine import Engine
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--config", default="p1_tc_chung_lu_small", choices=sorted(graphs.CONFIGS))
+    ap.add_argument("--config", default="tc_chung_lu_40k", choices=sorted(graphs.CONFIGS))
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--repeats", type=int, default=2)
     ap.add_argument("--out", default="")

@@ -126,15 +126,15 @@ def batched_workload(count: int = 1024, lo: int = 1000, hi: int = 200_000, seed:
 
 CONFIGS = {
     # name: (program, generator, kwargs)
-    "c0_tc_dag": ("tc", dag, {}),
-    "c1_tc_chung_lu": ("tc", chung_lu, {}),
-    "c2_sg_lattice": ("sg", lattice3d, {}),
+    "tc_dag_5k": ("tc", dag, {}),
+    "tc_chung_lu_317k": ("tc", chung_lu, {}),
+    "sg_lattice_55": ("sg", lattice3d, {}),
     # the TC-at-scale shape at 1/8 of the nodes (~3e7 closure tuples, a few
     # hundred MB: larger than L2, small enough for detailed counter captures)
-    "p1_tc_chung_lu_small": ("tc", chung_lu, {"n": 40_000, "m": 132_500}),
+    "tc_chung_lu_40k": ("tc", chung_lu, {"n": 40_000, "m": 132_500}),
     # 1/4 of the nodes (~1e8 closure tuples, ~4 GB on the device): join steps
     # of milliseconds for counter captures of the bit-matrix step
-    "p2_tc_chung_lu_medium": ("tc", chung_lu, {"n": 80_000, "m": 265_000}),
+    "tc_chung_lu_80k": ("tc", chung_lu, {"n": 80_000, "m": 265_000}),
 }
 
 

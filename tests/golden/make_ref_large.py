@@ -52,7 +52,7 @@ CASES = [
     ("ca_hepth_sg", "sg", "data_51971.bin", (74_618_689, 9), "logs/small-merged-job-output.txt:250"),
     ("ego_facebook_sg", "sg", "data_88234.bin", (15_018_986, 13), "logs/small-merged-job-output.txt:269"),
     ("fe_ocean_sg", "sg", "data_409593.bin", (65_941_441, 77), "README.md:54"),
-    ("c1_tc_chung_lu", "tc", "synthetic:c1_tc_chung_lu", None, None),
+    ("tc_chung_lu_317k", "tc", "synthetic:tc_chung_lu_317k", None, None),
     # single_join's synthetic rows (glibc srand(1)/rand(), common/parallel_io.cu:79-108): the weak- and
     # strong-scaling inputs of one rank; the reference never writes this program's output file (job_run
     # is fixed at 1, single_join.cu:78), so these are pinned by counts

@@ -49,6 +49,6 @@ def test_combine_ranks_single_process():
 
 def test_reference_arm_only_on_rank_zero(capsys):
     import bench
-    args = argparse.Namespace(warmup=1, steps=1, config="c1_tc_chung_lu")
+    args = argparse.Namespace(warmup=1, steps=1, config="tc_chung_lu_317k")
     assert bench.main_reference(args, rank=1, world=2) == 0
     assert capsys.readouterr().out == ""  # rank 1 does no work and prints nothing
