@@ -9,9 +9,10 @@
 // goes from 0 to 1. The delta is the same set as the reference's (every new
 // bit is claimed by exactly one atomic on M), so per-iteration |delta| and the
 // fixpoint are identical. The result rows leave in the reference's output
-// order (tc.cu:345-366: by target, then source) straight from M's columns:
-// a counting pass and a rows pass over M, each transposing 32 x 32 bit
-// blocks in registers.
+// order (tc.cu:345-366: by target, then source) from M's transpose, made by
+// one pass over M that transposes 32 x 32 bit blocks in registers, or --
+// when a second matrix does not fit -- straight from M's columns by a
+// counting pass and a rows pass of the same kind.
 //
 // A delta is kept as units: one source x and a run of path targets y (u32,
 // at most `unit_rows` of them; Tuning::bitmap_unit_rows, default 65,536: a
@@ -715,16 +716,18 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // TC's result rows (x, z) in the reference's order (by z, then x) come from
-// the columns of the matrix M (row x, bit z). Two passes walk M in tiles of
-// CX_ROWS source rows x CX_WORDS column words (128 bytes of every row, read
-// with 16-byte cp.async into shared memory, the next tile in flight while
-// the current one is worked on):
-//   count pass: per tile and target z, the set bits of column z in the
-//     tile's rows -> off[xb][z] (xb = the tile's row block);
-//   a column scan turns off[.][z] into offsets within column z, a scan of
+// the columns of the matrix M (row x, bit z). Each pass below walks M in
+// tiles of CX_ROWS source rows x CX_WORDS column words (128 bytes of every
+// row, read with 16-byte cp.async into shared memory, the next tile in
+// flight while the current one is worked on):
+//   transpose pass (the default form): each tile's target-major words are
+//     stored as 64-byte segments of T (row = target) with per-target counts;
+//   count pass (column form): per tile and target z, the set bits of column
+//     z in the tile's rows -> off[xb][z] (xb = the tile's row block); a
+//     column scan turns off[.][z] into offsets within column z, a scan of
 //     the column totals gives each z its first row;
-//   rows pass: the same walk writes every set bit (x, z) of a tile to
-//     out[first[z] + off[xb][z] + rank of x among the tile's bits of z].
+//   rows pass (column form): the same walk writes every set bit (x, z) of a
+//     tile to out[first[z] + off[xb][z] + rank of x among the tile's bits].
 // In a tile, thread (warp w, lane l) reads the 32 x 32 bit block (row block
 // rb = l % 16, column word cw = (w + l) % 32) one row at a time -- the 32
 // lanes read 32 different column words, so no bank conflicts -- transposes

@@ -504,7 +504,7 @@ static void run_tc_impl(Context &ctx, Run &r, const int32_t *rows_in, u64 n, boo
         u64 *e = sort_unique_into(ctx, ws.w0, ws.w1, n, 2 * g.bits, ne);
         build_csr(ctx, e, ne, g);
         if (dense || bitmat_choose(ctx, opt, g.n_ids, false)) {
-            nfull = tc_bitmap_fixpoint(ctx, r, g, e, ne, opt, pt);  // result: the matrix and its column offsets, in r
+            nfull = tc_bitmap_fixpoint(ctx, r, g, e, ne, opt, pt);  // result: the transpose, or the matrix and column offsets, in r
             cur = 0;
         } else {
             u64 nd;
