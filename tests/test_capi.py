@@ -71,3 +71,22 @@ def test_oracle_ops_restatement_basics():
     assert ops.set_difference(ops.sort_unique(a), b).tolist() == [[-1, 5], [1, -4], [3, 1]]
     assert ops.join(np.array([[1, 5], [1, 6], [2, 7]]), np.array([[1, 9], [3, 0], [2, 8]])).tolist() == \
         [[5, 9], [6, 9], [7, 8]]
+
+
+def test_profile_classes_match_the_ncu_summary_classes():
+    """Every kernel class of the library's live profile (dl_context.cu) is a
+    class the ncu launch-list summary (mnmgdatalog_b200/profiling.py) can
+    attribute kernels to, and the summary names no class the library lacks,
+    so the committed launch lists and the bench's profile speak of the same
+    classes."""
+    import re
+
+    from mnmgdatalog_b200 import profiling
+    src = open(os.path.join(ROOT, "mnmgdatalog_b200", "csrc", "dl_context.cu")).read()
+    block = src[src.index("static const char *names[K_COUNT]"):]
+    block = block[:block.index("};")]
+    lib_classes = {c for c in re.findall(r'"([a-z_A-Z]+)"', block) if not c.startswith("host_")}
+    ncu_classes = {cls for _, cls in profiling.CLASSES} | {"prep"}
+    assert ncu_classes <= lib_classes, sorted(ncu_classes - lib_classes)
+    # a class with no pattern would have its kernels counted as "prep" in the summary
+    assert not lib_classes - ncu_classes, sorted(lib_classes - ncu_classes)
