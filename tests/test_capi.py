@@ -90,3 +90,24 @@ def test_profile_classes_match_the_ncu_summary_classes():
     assert ncu_classes <= lib_classes, sorted(ncu_classes - lib_classes)
     # a class with no pattern would have its kernels counted as "prep" in the summary
     assert not lib_classes - ncu_classes, sorted(lib_classes - ncu_classes)
+
+
+@pytest.mark.parametrize("lang,std", [("c", "-std=c99"), ("c++", "-std=c++17")])
+def test_public_header_compiles_as_plain_c_and_cpp(tmp_path, lang, std):
+    """include/mnmgdl.h is usable from C (cgo, FFI generators) and C++ alike:
+    it compiles with -pedantic and every warning enabled."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    src = tmp_path / ("use." + ("c" if lang == "c" else "cpp"))
+    src.write_text('#include "mnmgdl.h"\n'
+                   "int main(void) {\n"
+                   "    dl_tuning t; dl_options o; dl_run_info i; dl_kernel_stat k;\n"
+                   "    (void) t; (void) o; (void) i; (void) k;\n"
+                   "    return dl_status_string(DL_OK) == 0;\n"
+                   "}\n")
+    r = subprocess.run([cc, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                        "-I", os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
