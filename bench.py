@@ -505,12 +505,30 @@ def measure_sg_dataset(eng, args, dev, flush) -> dict:
     steps = max(1, min(args.steps, 3))
     ms, r, prof = timed_fixpoints(eng, "sg", d_edges, steps, 1, "auto", dev, 1, lambda: None, flush)
     roofline, kernels, _, launches = roofline_of(prof, sum(ms) / 1e3)
+    cpu = None if args.no_cpu_baseline else sg_cpu_sample()
     return {"workload": f"SG on {name} ({fname}, {len(edges)} edges; the reference published {pub_tuples} tuples "
                         f"in {pub_iters} iterations, {cite})",
             "value": r.output_tuples * steps / (sum(ms) / 1e3), "unit": UNIT, "steps": steps,
             "ms_per_step": sum(ms) / steps, "tuples": int(r.output_tuples), "iterations": int(r.iterations),
             "matches_published": bool(r.output_tuples == pub_tuples and r.iterations == pub_iters),
-            "roofline": roofline, "kernels": kernels, "gpu_launches": launches, "reference_gpu": ref}
+            "roofline": roofline, "kernels": kernels, "gpu_launches": launches, "reference_gpu": ref,
+            "cpu_baseline": cpu}
+
+
+def sg_cpu_sample() -> dict:
+    """SG on the host cores: the reference has no CPU SG program, so the
+    oracle's single-core restatement of sg.cu is timed (project code, labelled
+    "port") on a bounded sample -- the small lattice of the SG generator
+    (4,702 edges, 4.4M SG tuples, a few seconds)."""
+    from oracle import cpu as oracle_cpu
+    e = load_fixture("synth_lattice_small.bin")
+    t0 = time.perf_counter()
+    r = oracle_cpu.sg(e)
+    sec = time.perf_counter() - t0
+    return {"value": len(r.rows) / sec, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"SG of the small lattice (tests/golden/data/synth_lattice_small.bin, {len(e)} edges): "
+                      f"{len(r.rows)} tuples in {r.iterations} iterations, {sec:.2f} s, the oracle's C restatement "
+                      f"of sg.cu on one core (the reference has no CPU SG program)"}
 
 
 def traffic_per_launch(kernel: str, stat: dict):
